@@ -1,0 +1,231 @@
+/*
+ * pipeflow_b200.h -- C ABI of the B200 (sm_100a) timestep hot path of the
+ * openpipeflow pipe-flow DNS (Fortran 90 reference, openpipeflow 1.12).
+ *
+ * Every entry point returns an int status: PF_OK (0) or a negative PF_ERR_*
+ * code; pf_last_error() gives the message of the calling thread's last
+ * failure.  A Fortran ISO_C_BINDING shim maps a non-zero status to
+ * `stop <message>`, which is the reference's error behaviour for every
+ * failure (e.g. timestep.f90:93,117, meshs.f90:238).
+ *
+ * Object model (one pf_ctx per pipe == the module state of the reference's
+ * modules variables/transform/timestep/velocity for one run):
+ *   pf_ctx     parameters.f90 + module state (tim_*, vel_*, matrices)
+ *   pf_coll    one `type (coll)` field on the device       (variables.f90:37-40)
+ *   pf_phys    one `type (phys)` field on the device       (variables.f90:42-44)
+ *   pf_mesh    one set of per-mode `type (mesh)` band matrices (meshs.f90:37-39)
+ *   pf_lumesh  one set of per-mode `type (lumesh)` LU factors (meshs.f90:42-45)
+ *
+ * Host-array layouts follow the reference exactly (Fortran column-major):
+ *   coll: re[nh*N + n], im[nh*N + n]        == %Re(n+1, nh), %Im(n+1, nh)
+ *   phys: re[(n*Th + t)*Z + z]              == %Re(z, t, n+1)
+ *   mesh: M[(nh*N + j)*(2KL+1) + row]       == A(nh)%M(row+1, j+1)
+ *   lumesh: M[(nh*N + j)*(3KL+1) + row], ipiv[nh*N + j] (1-based, LAPACK)
+ * with the harmonic order of the serial _loop_km macro (parallel.h:47-57):
+ * nh = m*(2K-1)+k, m = 0..M-1, k = -(K-1)..K-1, skipping k<0 when m=0.
+ *
+ * Calls are asynchronous on the context's CUDA stream unless they return a
+ * host value (norms, corrector error, CFL, downloads), which synchronise it.
+ * A context is not thread-safe; separate contexts may be used concurrently.
+ */
+#ifndef PIPEFLOW_B200_H
+#define PIPEFLOW_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PF_OK            0
+#define PF_ERR_ARG      -1   /* bad argument / size mismatch                */
+#define PF_ERR_CUDA     -2   /* CUDA runtime failure                        */
+#define PF_ERR_SINGULAR -3   /* zero pivot in a banded or 4x4 factorisation */
+#define PF_ERR_NOMEM    -4   /* device allocation failed / over budget      */
+#define PF_ERR_STATE    -5   /* call out of order (e.g. step before matrices) */
+#define PF_ERR_CONVERGE -6   /* corrector diverged / too many iterations    */
+#define PF_ERR_NODEVICE -7   /* no CUDA device visible                      */
+
+#define PF_KL 4              /* i_KL, parameters.f90:43 */
+
+/* precision of the transform / nonlinear-product stage */
+#define PF_PREC_FP64  0      /* everything FP64 (the reference's arithmetic) */
+#define PF_PREC_MIXED 1      /* FP32 FFTs and u x curl(u); FP64 elsewhere    */
+
+/* Runtime replacement of the compile-time parameters (parameters.f90:15-51). */
+typedef struct pf_config {
+    int    N, K, M, Mp;          /* i_N, i_K, i_M, i_Mp                        */
+    double Re, alpha;            /* d_Re, d_alpha                              */
+    double dt;                   /* d_timestep (>0 fixed, <0 adaptive)         */
+    double implicit;             /* d_implicit (0.51)                          */
+    double dterr;                /* d_dterr    (1e-5)                          */
+    double courant;              /* d_courant  (0.5)                           */
+    double maxdt;                /* d_maxdt    (1e99)                          */
+    int    const_flux;           /* b_const_flux                               */
+    int    mirrorsym, shiftrefl, shiftrott;   /* b_mirrorsym, ...             */
+    const double *r;             /* custom radial mesh (mesh.in, meshs.f90:76-88); NULL = default */
+    int    precision;            /* PF_PREC_FP64 or PF_PREC_MIXED              */
+} pf_config;
+
+/* Timestep module scalars (timestep.f90:12-21). */
+typedef struct pf_tim_state {
+    double t, dt, dterr, corr_dt, cfl_dt;
+    int    it, step, cfl_dir, new_dt, pcn;
+} pf_tim_state;
+
+typedef struct pf_ctx    pf_ctx;
+typedef struct pf_coll   pf_coll;
+typedef struct pf_phys   pf_phys;
+typedef struct pf_mesh   pf_mesh;
+typedef struct pf_lumesh pf_lumesh;
+
+/* ---------------------------------------------------------------- context */
+const char *pf_last_error(void);
+int pf_version(int *major, int *minor);
+/* par_precompute + mes_precompute + var_precompute + tra_precompute +
+ * tim_precompute + vel_precompute (main.f90:109-114; parameters.f90:59-62;
+ * meshs.f90:66-103; variables.f90:60-88; transform.fftw3.f90:35-59;
+ * timestep.f90:29-40; velocity.f90:47-55).  device < 0 keeps the current one. */
+int pf_ctx_create(const pf_config *cfg, int device, pf_ctx **out);
+int pf_ctx_destroy(pf_ctx *ctx);
+/* Run the context's work on an external cudaStream_t (NULL = own stream). */
+int pf_ctx_set_stream(pf_ctx *ctx, void *cuda_stream);
+int pf_ctx_sync(pf_ctx *ctx);
+/* H = number of harmonics (i_H1+1), Z = 3K, Th = 3M. */
+int pf_ctx_dims(const pf_ctx *ctx, int *N, int *H, int *Z, int *Th);
+/* Bytes of device memory held by the context (fields, factors, scratch). */
+int pf_ctx_device_bytes(const pf_ctx *ctx, unsigned long long *bytes);
+
+/* Radial mesh `mes_D` (meshs.f90:48-58): r(N), dr(KL) bands [(i*N+j)*(2KL+1)+row],
+ * radLap band, dr0/dr1 [(i*(KL+1))+j] == dr0(j+1,i), intrdr(N).  Any pointer may be NULL. */
+int pf_mes_get(const pf_ctx *ctx, double *r, double *dr, double *radLap,
+               double *dr0, double *dr1, double *intrdr);
+/* The same mesh computed on the host only (no device needed): mes_precompute
+ * + mes_rdom_init (meshs.f90:66-194) for N points; custom_r may be NULL. */
+int pf_mes_compute(int N, const double *custom_r, double *r, double *dr,
+                   double *radLap, double *dr0, double *dr1, double *intrdr);
+
+/* ----------------------------------------------------------------- fields */
+int pf_coll_create(pf_ctx *ctx, pf_coll **out);
+int pf_coll_destroy(pf_coll *c);
+int pf_coll_upload(pf_coll *c, const double *re, const double *im);
+int pf_coll_download(const pf_coll *c, double *re, double *im);
+int pf_phys_create(pf_ctx *ctx, pf_phys **out);
+int pf_phys_destroy(pf_phys *p);
+int pf_phys_upload(pf_phys *p, const double *re);
+int pf_phys_download(const pf_phys *p, double *re);
+
+/* --------------------------------------------------------- variables.f90 */
+int pf_var_coll_init(pf_coll *a);                                   /* :118-122 */
+int pf_var_coll_copy(const pf_coll *in, pf_coll *out);              /* :128-133 */
+int pf_var_coll_add(const pf_coll *ac, pf_coll *a);                 /* :139-144 */
+int pf_var_coll_sub(const pf_coll *ac, pf_coll *a);                 /* :150-155 */
+int pf_var_coll_dmult(double d, pf_coll *a);                        /* :161-166 */
+int pf_var_coll_neg(const pf_coll *ac, pf_coll *a);                 /* :172-177 */
+/* out = mes_D%dr(p) . in  (p = 1..KL) */
+int pf_var_coll_meshmult(int p, const pf_coll *in, pf_coll *out);   /* :378-402 */
+int pf_var_coll_curl(const pf_coll *r, const pf_coll *t, const pf_coll *z,
+                     pf_coll *or_, pf_coll *ot, pf_coll *oz);       /* :408-436 */
+int pf_var_coll_grad(const pf_coll *p, pf_coll *r, pf_coll *t, pf_coll *z); /* :442-459 */
+int pf_var_coll_div(const pf_coll *r, const pf_coll *t, const pf_coll *z,
+                    pf_coll *dv);                                   /* :465-481 */
+int pf_var_coll_shift(double dt, double dz, const pf_coll *a, pf_coll *b); /* :487-528 */
+int pf_var_imposesym(int i, pf_coll *r, pf_coll *t, pf_coll *z);    /* :538-618 */
+/* E and the spectra Ek(0:K-1), Em(0:M-1) (either may be NULL) */
+int pf_var_coll_norm(const pf_coll *a, double *E, double *Ek, double *Em); /* :718-751 */
+
+/* -------------------------------------------------- transform.fftw3.f90 */
+/* var_coll2spec + tra_spec2phys (variables.f90:184-197, transform.fftw3.f90:65-102) */
+int pf_tra_coll2phys(const pf_coll *c, pf_phys *p);
+/* tra_phys2spec + var_spec2coll (transform.fftw3.f90:108-147, variables.f90:281-294) */
+int pf_tra_phys2coll(const pf_phys *p, pf_coll *c);
+
+/* ---------------------------------------------------------- timestep.f90 */
+int pf_tim_get(const pf_ctx *ctx, pf_tim_state *s);
+int pf_tim_set(pf_ctx *ctx, const pf_tim_state *s);
+/* A = c1 I + c2 Lap(PM) per mode (timestep.f90:46-60) */
+int pf_tim_mesh_init(pf_ctx *ctx, int PM, double c1, double c2, pf_mesh **out);
+int pf_mesh_destroy(pf_mesh *A);
+int pf_mesh_download(const pf_mesh *A, double *M);
+/* Same matrix with axis-parity / wall rows, banded LU with partial pivoting
+ * (dgbtrf semantics), skipped for BC=1 at k=m=0 (timestep.f90:67-96) */
+int pf_tim_lumesh_init(pf_ctx *ctx, int PM, int BC, double c1, double c2, pf_lumesh **out);
+int pf_lumesh_destroy(pf_lumesh *A);
+int pf_lumesh_download(const pf_lumesh *A, double *M, int *ipiv);
+/* b := A^-1 b per mode, Re and Im (dgbtrs semantics; zero for BC=1,k=m=0)
+ * (timestep.f90:102-123) */
+int pf_tim_lumesh_invert(int BC, const pf_lumesh *A, pf_coll *b);
+/* d = A b + c (timestep.f90:130-154); d may alias b or c */
+int pf_tim_meshmult(int S, const pf_mesh *A, const pf_coll *b, const pf_coll *c, pf_coll *d);
+int pf_tim_zerobc(pf_coll *a);                                      /* :160-169 */
+int pf_tim_nlincorr(const pf_coll *N_, pf_coll *Nn);                /* :174-184 */
+int pf_tim_measurecorr(const pf_coll *c1, const pf_coll *c2, const pf_coll *c3); /* :190-207 */
+int pf_tim_check_cgce(pf_ctx *ctx);                                 /* :214-253 */
+int pf_tim_new_tstep(pf_ctx *ctx);                                  /* :259-278 */
+
+/* ---------------------------------------------------------- velocity.f90 */
+/* Module fields: 0..2 vel_ur,vel_ut,vel_uz; 3..5 vel_Nr,vel_Nt,vel_Nz (coll);
+ * physical 0..5 vel_r,vel_t,vel_z,vel_curlr,vel_curlt,vel_curlz. */
+#define PF_UR 0
+#define PF_UT 1
+#define PF_UZ 2
+#define PF_NR 3
+#define PF_NT 4
+#define PF_NZ 5
+int pf_vel_coll(pf_ctx *ctx, int which, pf_coll **out);
+int pf_vel_phys(pf_ctx *ctx, int which, pf_phys **out);
+/* Host state in / out: vel_ur, vel_ut, vel_uz in the coll host layout. */
+int pf_vel_set_state(pf_ctx *ctx, const double *ur_re, const double *ur_im,
+                     const double *ut_re, const double *ut_im,
+                     const double *uz_re, const double *uz_im);
+int pf_vel_get_state(pf_ctx *ctx, double *ur_re, double *ur_im,
+                     double *ut_re, double *ut_im, double *uz_re, double *uz_im);
+int pf_vel_get_scalars(const pf_ctx *ctx, double *Pr0, double *nu);
+int pf_vel_imposesym(pf_ctx *ctx);                                  /* :61-74 */
+int pf_vel_matrices(pf_ctx *ctx);                                   /* :120-146 */
+int pf_vel_transform(pf_ctx *ctx);                                  /* :304-317 */
+int pf_vel_nonlinear(pf_ctx *ctx);                                  /* :323-335 */
+int pf_vel_predictor(pf_ctx *ctx);                                  /* :400-410 */
+int pf_vel_corrector(pf_ctx *ctx);                                  /* :416-432 */
+int pf_vel_maxtstep(pf_ctx *ctx);                                   /* :438-481 */
+/* Influence data of vel_adjPPE(0): U(N,nh,6) [(c*H+nh)*N+n] and the inverted
+ * 4x4 A(4,4,nh) [nh*16 + j*4 + i] == A(i+1,j+1,nh). */
+int pf_vel_influence_download(const pf_ctx *ctx, double *U, double *A);
+
+/* -------------------------------------------------------------- drivers */
+/* One pass of the main.f90 loop body (main.f90:20-44): imposesym, transform,
+ * nonlinear, [adaptive dt], predictor, corrector iterated until
+ * tim_check_cgce says converged.  *ncorr (may be NULL) = corrector passes.
+ * Returns PF_ERR_CONVERGE when tim_check_cgce reports divergence. */
+int pf_timestep(pf_ctx *ctx, int *ncorr);
+/* nsteps passes of steporbit's body (newton.f90:740-762): exactly one
+ * corrector per step, no adaptive dt, no shift. */
+int pf_steporbit(pf_ctx *ctx, int nsteps);
+/* Perturbation energy and friction diagnostics of io.f90:501-514, 627-639. */
+int pf_diag_energy(pf_ctx *ctx, double *E);
+int pf_diag_friction(pf_ctx *ctx, double *Ub, double *Uc, double *Ufr);
+
+/* ------------------------------------------------------- instrumentation */
+/* Kernel categories timed by CUDA events when profiling is on (the reference
+ * has only the CPU-time clk_time, main.f90:175-186). */
+#define PF_K_ZINV     0   /* z pass spectral -> (m,z) columns              */
+#define PF_K_THINV    1   /* theta pass (c2r) -> physical                   */
+#define PF_K_THFWD    2   /* theta pass (r2c), fused u x curl(u)            */
+#define PF_K_ZFWD     3   /* z pass -> spectral, truncation                 */
+#define PF_K_LUSOLVE  4   /* banded solves                                   */
+#define PF_K_STENCIL  5   /* meshmult / curl / grad / div / tim_meshmult    */
+#define PF_K_EW       6   /* elementwise, symmetry, reductions, transfers   */
+#define PF_K_INFL     7   /* influence correction, flux, addHPF             */
+#define PF_K_FACTOR   8   /* banded LU factorisation (vel_matrices)          */
+#define PF_K_STEP     9   /* fused per-mode step kernels                     */
+#define PF_K_NCAT    10
+/* Count of this library's kernel launches on the context since creation. */
+int pf_ctx_launches(const pf_ctx *ctx, unsigned long long *n);
+/* Enable (1) / disable (0) per-category event timing; enabling clears totals. */
+int pf_prof_enable(pf_ctx *ctx, int on);
+/* Total device milliseconds and launches of category `cat` since enabling
+ * (synchronises the stream). */
+int pf_prof_read(pf_ctx *ctx, int cat, double *ms, unsigned long long *launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PIPEFLOW_B200_H */

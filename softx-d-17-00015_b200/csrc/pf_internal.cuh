@@ -1,0 +1,247 @@
+// Internal definitions shared by the pipeflow_b200 translation units.
+//
+// Device data layout (all FP64 unless noted):
+//   coll field  : double2 d[n*Hp + nh]   (complex, harmonic index fastest, row
+//                 pitch Hp = H rounded up to 32).  The reference's coll type is
+//                 (n fastest); storing the harmonic index fastest makes the
+//                 per-radial-point transform tiles contiguous and keeps the
+//                 per-mode solves coalesced across modes, so the reference's
+//                 coll<->spec transposes (variables.f90:184-370) vanish on the
+//                 device.  Host<->device copies reorder once.
+//   phys field  : double d[(n*Th + t)*Z + z]  (identical to the reference)
+//   LU factors  : double lu[(row*N + col)*Hp + nh], row = LAPACK band row-1
+//                 (0..3KL), pivots uint8 piv[col*Hp + nh] = ipiv-col (0..KL)
+//   FFT scratch : complex T[((c*N + n)*M + m)*Z + z]
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <string>
+#include <vector>
+#include "pipeflow_b200.h"
+
+#define KL PF_KL
+#define KV (2 * PF_KL)          // LAPACK KV = KU+KL
+#define NBAND (2 * PF_KL + 1)   // rows of a mesh band
+#define NLU (3 * PF_KL + 1)     // rows of a lumesh band (LDAB)
+
+// ------------------------------------------------------------------ errors
+void pf_set_error(const char *fmt, ...);
+#define PF_CUDA(call)                                                        \
+    do {                                                                     \
+        cudaError_t e_ = (call);                                             \
+        if (e_ != cudaSuccess) {                                             \
+            pf_set_error("%s:%d %s: %s", __FILE__, __LINE__, #call,          \
+                         cudaGetErrorString(e_));                            \
+            return PF_ERR_CUDA;                                              \
+        }                                                                    \
+    } while (0)
+#define PF_CHECK_LAUNCH() PF_CUDA(cudaGetLastError())
+#define PF_TRY(expr)                                                         \
+    do {                                                                     \
+        int s_ = (expr);                                                     \
+        if (s_ != PF_OK) return s_;                                          \
+    } while (0)
+#define PF_ARG(cond, msg)                                                    \
+    do {                                                                     \
+        if (!(cond)) {                                                       \
+            pf_set_error("%s", msg);                                         \
+            return PF_ERR_ARG;                                               \
+        }                                                                    \
+    } while (0)
+
+// ---------------------------------------------------------------- geometry
+struct Geo {
+    int N, K, M, Mp, H, Hp, Z, Th;
+    double alpha, Re;
+};
+
+// harmonic index -> (k, m): inverse of nh = m*(2K-1)+k (parallel.h:27-38)
+__host__ __device__ inline void mode_km(int nh, int K, int &k, int &m) {
+    if (nh < K) {
+        m = 0;
+        k = nh;
+    } else {
+        m = (nh + K - 1) / (2 * K - 1);
+        k = nh - m * (2 * K - 1);
+    }
+}
+
+// Radial mesh on the device (meshs.f90:48-55).
+struct DevMesh {
+    const double *rp;      // r^j, j=-3..3: rp[(j+3)*N + n]
+    const double *dr;      // dr(1..KL) bands: dr[((p-1)*NBAND + row)*N + col]
+    const double *radLap;  // [row*N + col]
+    const double *dr0;     // dr0[i*(KL+1) + j] == dr0(j+1, i)
+    const double *dr1;     // dr1[i*(KL+1) + j] == dr1(j+1, i)
+    const double *intrdr;  // [n]
+    const double *velU;    // 1 - r^2
+    const double *velUp;   // -2 r
+};
+
+// Host copy of the mesh (same layouts as DevMesh).
+struct HostMesh {
+    std::vector<double> r, rp, dr, radLap, dr0, dr1, intrdr;
+};
+int pf_build_mesh(int N, const double *custom_r, HostMesh &hm);
+
+// Device scalars of one context.
+struct DevScalars {
+    double Pr0;                      // vel_Pr0
+    double flux_d1;                  // vel_adjustFlux d1
+    unsigned long long dterr2_bits;  // max |corr|^2 as ordered bits
+    int info;                        // first singular pivot (1-based col), 0 = ok
+    int pad;
+};
+
+// Mixed-radix FFT plan of length L: radices in application order.
+struct FFTPlan {
+    int L, nf;
+    int f[16];
+};
+int pf_make_plan(int L, FFTPlan &p);
+
+struct pf_ctx;
+
+struct pf_coll {
+    pf_ctx *ctx;
+    double2 *d;
+};
+struct pf_phys {
+    pf_ctx *ctx;
+    double *d;
+};
+struct pf_mesh {
+    pf_ctx *ctx;
+    int PM;
+    double c1, c2;
+};
+struct pf_lumesh {
+    pf_ctx *ctx;
+    int PM, BC;
+    double c1, c2;
+    double *lu;
+    unsigned char *piv;
+};
+
+struct pf_ctx {
+    pf_config cfg;
+    Geo g;
+    int device;
+    cudaStream_t stream;
+    bool own_stream;
+    HostMesh hm;
+    DevMesh dm;
+    double *dmesh_mem;  // backing store of dm
+    FFTPlan planZ, planT;
+    double2 *twZ, *twT;  // exp(+2 pi i t/L), t=0..L-1, FP64
+    float2 *twZf, *twTf; // same in FP32 (mixed precision)
+    DevScalars *dsc;     // device scalars
+    DevScalars *hsc;     // pinned host mirror
+    unsigned long long bytes;
+    // timestep module (timestep.f90:12-21)
+    pf_tim_state tim;
+    double lasterr;
+    int newdt_i;
+    // velocity module (velocity.f90:14-39)
+    pf_coll vel[6];      // ur ut uz Nr Nt Nz
+    pf_coll prev[6];     // ur_ ut_ uz_ Nr_ Nt_ Nz_
+    pf_coll save[3];     // corrector's r,t,z copies
+    pf_coll s[8];        // scratch
+    pf_phys phys[6];     // vel_r .. vel_curlz
+    pf_lumesh LNp, LDp, LDm, LDz;
+    pf_mesh Ltp, Ltm, Ltz;
+    bool LNp_set, matrices_ready;
+    double vel_nu;
+    double *U;           // influence solutions [(c*N + n)*Hp + nh], c=0..5
+    double *Ainv;        // inverted 4x4 [(i*4+j)*Hp + nh] == A(i+1,j+1,nh)
+    double *Ui;          // flux influence vector [N]
+    double *red;         // reduction scratch (>= 3*N + H doubles)
+    void *T;             // FFT scratch: 6*N*M*Z complex (FP64)
+    size_t T_bytes;
+    int zinv_mc, zfwd_mc, th_zc;   // tile sizes
+    std::vector<void *> allocs;    // everything to free
+    // instrumentation
+    unsigned long long launches;
+    bool prof_on;
+    std::vector<cudaEvent_t> ev_pool;                 // free events
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_open[PF_K_NCAT];
+    double prof_ms[PF_K_NCAT];
+    unsigned long long prof_n[PF_K_NCAT];
+};
+
+// Records a start/stop event pair around the launches in its scope when
+// profiling is enabled on the context.
+cudaEvent_t pf_event_get(pf_ctx *ctx);
+struct ProfScope {
+    pf_ctx *ctx;
+    int cat;
+    cudaEvent_t a;
+    ProfScope(pf_ctx *c, int k) : ctx(c), cat(k), a(nullptr) {
+        if (ctx->prof_on) {
+            a = pf_event_get(ctx);
+            cudaEventRecord(a, ctx->stream);
+        }
+    }
+    ~ProfScope() {
+        if (a) {
+            cudaEvent_t b = pf_event_get(ctx);
+            cudaEventRecord(b, ctx->stream);
+            ctx->ev_open[cat].push_back({a, b});
+        }
+    }
+};
+#define PF_LAUNCHED(ctx)     \
+    do {                     \
+        (ctx)->launches++;   \
+        PF_CHECK_LAUNCH();   \
+    } while (0)
+
+// -------------------------------------------------------------- utilities
+int pf_alloc(pf_ctx *ctx, void **p, size_t bytes);
+int pf_coll_init_storage(pf_ctx *ctx, pf_coll *c);
+int pf_phys_init_storage(pf_ctx *ctx, pf_phys *p);
+inline double bits_to_double(unsigned long long b) {
+    double d;
+    std::memcpy(&d, &b, sizeof(d));
+    return d;
+}
+inline unsigned grid1(long long n, int block) {
+    return (unsigned)((n + block - 1) / block);
+}
+
+// launchers implemented in the .cu files (all on ctx->stream)
+enum EwOp {
+    EW_ZERO, EW_COPY, EW_ADD, EW_SUB, EW_NEG, EW_DMULT, EW_RT2PM, EW_PM2RT,
+    EW_NLINCORR, EW_SUBFROM
+};
+int pf_launch_ew(pf_ctx *ctx, EwOp op, const double2 *a, const double2 *b,
+                 double2 *o1, double2 *o2, double s);
+int pf_launch_zerobc(pf_ctx *ctx, double2 *a);
+int pf_launch_meshmult_dr(pf_ctx *ctx, int p, const double2 *in, double2 *out);
+int pf_launch_curl(pf_ctx *ctx, const double2 *r, const double2 *t, const double2 *z,
+                   double2 *or_, double2 *ot, double2 *oz);
+int pf_launch_grad(pf_ctx *ctx, const double2 *p, double2 *r, double2 *t, double2 *z);
+int pf_launch_div(pf_ctx *ctx, const double2 *r, const double2 *t, const double2 *z,
+                  double2 *dv);
+int pf_launch_tim_meshmult(pf_ctx *ctx, const pf_mesh *A, const double2 *b,
+                           const double2 *c, double2 *d);
+int pf_launch_imposesym(pf_ctx *ctx, int i, double2 *r, double2 *t, double2 *z);
+int pf_launch_measurecorr(pf_ctx *ctx, const double2 *a0, const double2 *b0,
+                          const double2 *a1, const double2 *b1,
+                          const double2 *a2, const double2 *b2, bool reset);
+int pf_launch_addHPF(pf_ctx *ctx);
+int pf_launch_lu_factor(pf_ctx *ctx, pf_lumesh *A);
+int pf_launch_lu_solve(pf_ctx *ctx, int BC, const pf_lumesh *A, double2 *b);
+int pf_launch_adjppe2(pf_ctx *ctx);
+int pf_launch_flux1(pf_ctx *ctx);
+int pf_launch_zero_mode0(pf_ctx *ctx);
+int pf_vel_matrices_impl(pf_ctx *ctx);
+int pf_launch_coll2phys(pf_ctx *ctx, int ncomp, const double2 *const *src,
+                        double *const *dst);
+int pf_launch_phys2coll(pf_ctx *ctx, int ncomp, const double *const *src,
+                        double2 *const *dst, bool cross);
+int pf_launch_maxtstep(pf_ctx *ctx, double *dt3);
+int pf_norm_host(pf_ctx *ctx, const double2 *a, double *E, double *Ek, double *Em);

@@ -1,0 +1,275 @@
+// Velocity module and drivers: vel_transform / vel_nonlinear / vel_step /
+// predictor / corrector, corrector control and adaptive dt, and the main-loop
+// and steporbit step drivers (velocity.f90:61-481; timestep.f90:214-278;
+// main.f90:20-44; newton.f90:740-762).
+#include <cmath>
+#include "pf_internal.cuh"
+
+static int require_matrices(pf_ctx *ctx) {
+    if (!ctx->matrices_ready) {
+        pf_set_error("vel_matrices has not been called for this context");
+        return PF_ERR_STATE;
+    }
+    return PF_OK;
+}
+
+extern "C" int pf_vel_imposesym(pf_ctx *ctx) {
+    PF_ARG(ctx, "null ctx");
+    double2 *r = ctx->vel[0].d, *t = ctx->vel[1].d, *z = ctx->vel[2].d;
+    PF_TRY(pf_launch_imposesym(ctx, 0, r, t, z));
+    if (ctx->cfg.mirrorsym) PF_TRY(pf_launch_imposesym(ctx, 1, r, t, z));
+    if (ctx->cfg.shiftrefl) PF_TRY(pf_launch_imposesym(ctx, 2, r, t, z));
+    if (ctx->cfg.shiftrott) PF_TRY(pf_launch_imposesym(ctx, 3, r, t, z));
+    return PF_OK;
+}
+
+extern "C" int pf_vel_matrices(pf_ctx *ctx) {
+    PF_ARG(ctx, "null ctx");
+    return pf_vel_matrices_impl(ctx);
+}
+
+// u and curl(u) to physical space (velocity.f90:304-317)
+extern "C" int pf_vel_transform(pf_ctx *ctx) {
+    PF_ARG(ctx, "null ctx");
+    PF_TRY(pf_launch_curl(ctx, ctx->vel[0].d, ctx->vel[1].d, ctx->vel[2].d, ctx->s[0].d, ctx->s[1].d,
+                          ctx->s[2].d));
+    const double2 *src[6] = {ctx->vel[0].d, ctx->vel[1].d, ctx->vel[2].d, ctx->s[0].d, ctx->s[1].d, ctx->s[2].d};
+    double *dst[6];
+    for (int i = 0; i < 6; ++i) dst[i] = ctx->phys[i].d;
+    return pf_launch_coll2phys(ctx, 6, src, dst);
+}
+
+// u x curl(u), forward transforms, background-flow terms (velocity.f90:323-361)
+extern "C" int pf_vel_nonlinear(pf_ctx *ctx) {
+    PF_ARG(ctx, "null ctx");
+    const double *src[6];
+    for (int i = 0; i < 6; ++i) src[i] = ctx->phys[i].d;
+    double2 *dst[3] = {ctx->vel[3].d, ctx->vel[4].d, ctx->vel[5].d};
+    PF_TRY(pf_launch_phys2coll(ctx, 3, src, dst, true));
+    return pf_launch_addHPF(ctx);
+}
+
+// velocity.f90:367-394
+static int vel_step(pf_ctx *ctx) {
+    PF_TRY(require_matrices(ctx));
+    double2 *ur = ctx->vel[0].d, *ut = ctx->vel[1].d, *uz = ctx->vel[2].d;
+    double2 *Nr = ctx->vel[3].d, *Nt = ctx->vel[4].d, *Nz = ctx->vel[5].d;
+    double2 *s0 = ctx->s[0].d, *s1 = ctx->s[1].d, *s2 = ctx->s[2].d, *s3 = ctx->s[3].d;
+    double2 *s4 = ctx->s[4].d, *s5 = ctx->s[5].d;
+    // rhs = A u_ + N
+    PF_TRY(pf_launch_ew(ctx, EW_RT2PM, Nr, Nt, s0, s1, 0.0));
+    PF_TRY(pf_launch_ew(ctx, EW_RT2PM, ctx->prev[0].d, ctx->prev[1].d, s2, s3, 0.0));
+    PF_TRY(pf_launch_tim_meshmult(ctx, &ctx->Ltp, s2, s0, ur));
+    PF_TRY(pf_launch_tim_meshmult(ctx, &ctx->Ltm, s3, s1, ut));
+    PF_TRY(pf_launch_tim_meshmult(ctx, &ctx->Ltz, ctx->prev[2].d, Nz, uz));
+    // vel_adjPPE(1): pressure projection (velocity.f90:227-236)
+    PF_TRY(pf_launch_ew(ctx, EW_PM2RT, ur, ut, s0, s1, 0.0));
+    PF_TRY(pf_launch_div(ctx, s0, s1, uz, s2));
+    PF_TRY(pf_launch_zerobc(ctx, s2));
+    PF_TRY(pf_launch_lu_solve(ctx, 1, &ctx->LNp, s2));
+    PF_TRY(pf_launch_grad(ctx, s2, s3, s4, s5));
+    PF_TRY(pf_launch_ew(ctx, EW_RT2PM, s3, s4, s0, s1, 0.0));
+    PF_TRY(pf_launch_ew(ctx, EW_SUB, s0, nullptr, ur, nullptr, 0.0));
+    PF_TRY(pf_launch_ew(ctx, EW_SUB, s1, nullptr, ut, nullptr, 0.0));
+    PF_TRY(pf_launch_ew(ctx, EW_SUB, s5, nullptr, uz, nullptr, 0.0));
+    // invert
+    PF_TRY(pf_launch_zerobc(ctx, ur));
+    PF_TRY(pf_launch_zerobc(ctx, ut));
+    PF_TRY(pf_launch_zerobc(ctx, uz));
+    PF_TRY(pf_launch_lu_solve(ctx, 0, &ctx->LDp, ur));
+    PF_TRY(pf_launch_lu_solve(ctx, 0, &ctx->LDm, ut));
+    PF_TRY(pf_launch_lu_solve(ctx, 0, &ctx->LDz, uz));
+    PF_TRY(pf_launch_adjppe2(ctx));
+    PF_TRY(pf_launch_ew(ctx, EW_PM2RT, ur, ut, ur, ut, 0.0));
+    PF_TRY(pf_launch_flux1(ctx));
+    return pf_launch_zero_mode0(ctx);
+}
+
+// velocity.f90:400-410
+extern "C" int pf_vel_predictor(pf_ctx *ctx) {
+    PF_ARG(ctx, "null ctx");
+    for (int i = 0; i < 6; ++i)
+        PF_TRY(pf_launch_ew(ctx, EW_COPY, ctx->vel[i].d, nullptr, ctx->prev[i].d, nullptr, 0.0));
+    return vel_step(ctx);
+}
+
+// velocity.f90:416-432 (tim_measurecorr folded into one device reduction)
+static int vel_corrector_async(pf_ctx *ctx) {
+    for (int i = 0; i < 3; ++i)
+        PF_TRY(pf_launch_ew(ctx, EW_COPY, ctx->vel[i].d, nullptr, ctx->save[i].d, nullptr, 0.0));
+    for (int i = 3; i < 6; ++i)
+        PF_TRY(pf_launch_ew(ctx, EW_NLINCORR, ctx->prev[i].d, nullptr, ctx->vel[i].d, nullptr,
+                            ctx->cfg.implicit));
+    PF_TRY(vel_step(ctx));
+    return pf_launch_measurecorr(ctx, ctx->save[0].d, ctx->vel[0].d, ctx->save[1].d, ctx->vel[1].d,
+                                 ctx->save[2].d, ctx->vel[2].d, true);
+}
+
+static int read_dterr(pf_ctx *ctx) {
+    PF_CUDA(cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream));
+    PF_CUDA(cudaStreamSynchronize(ctx->stream));
+    const double d2 = bits_to_double(ctx->hsc->dterr2_bits);
+    ctx->tim.dterr = std::max(ctx->tim.dterr, std::sqrt(d2));
+    return PF_OK;
+}
+
+extern "C" int pf_vel_corrector(pf_ctx *ctx) {
+    PF_ARG(ctx, "null ctx");
+    PF_TRY(vel_corrector_async(ctx));
+    return read_dterr(ctx);
+}
+
+extern "C" int pf_vel_maxtstep(pf_ctx *ctx) {
+    PF_ARG(ctx, "null ctx");
+    double dt[3];
+    PF_TRY(pf_launch_maxtstep(ctx, dt));
+    ctx->tim.cfl_dt = std::min(dt[0], std::min(dt[1], dt[2]));
+    for (int i = 0; i < 3; ++i)
+        if (ctx->tim.cfl_dt == dt[i]) ctx->tim.cfl_dir = i + 1;
+    return PF_OK;
+}
+
+// timestep.f90:214-253; failures are reported as a status instead of
+// forcing the step counter to i_maxtstep-1
+extern "C" int pf_tim_check_cgce(pf_ctx *ctx) {
+    PF_ARG(ctx, "null ctx");
+    pf_tim_state &t = ctx->tim;
+    const pf_config &c = ctx->cfg;
+    int status = PF_OK;
+    if (t.it == 1) {
+        t.corr_dt = t.dterr > 0.0 ? t.dt * std::sqrt(c.dterr / t.dterr) : INFINITY;
+        ctx->lasterr = 1e99;
+    }
+    if (t.dt < 1e-9 && t.step > 30) {
+        pf_set_error("tim_check_cgce: dt --> 0 !!!?");
+        status = PF_ERR_CONVERGE;
+        t.it = 0;
+    } else if (t.it == t.pcn) {
+        t.it = 0;
+    } else if (t.it > 10) {
+        pf_set_error("tim_check_cgce: too many its!!!");
+        status = PF_ERR_CONVERGE;
+        t.it = 0;
+    } else if (t.dterr > ctx->lasterr) {
+        if (t.dterr > 2.0 * c.dterr) {
+            pf_set_error("tim_check_cgce: increasing error!!!");
+            status = PF_ERR_CONVERGE;
+        }
+        if (t.dterr < 2.0 * c.dterr) t.corr_dt = t.dt / (10.0 * c.courant);
+        t.it = 0;
+    } else if (t.dterr > c.dterr) {
+        ctx->lasterr = t.dterr;
+        t.it = t.it + 1;
+    } else {
+        t.it = 0;
+    }
+    t.dterr = 0.0;
+    return status;
+}
+
+// timestep.f90:259-278
+extern "C" int pf_tim_new_tstep(pf_ctx *ctx) {
+    PF_ARG(ctx, "null ctx");
+    pf_tim_state &t = ctx->tim;
+    const pf_config &c = ctx->cfg;
+    double dt = std::min(t.dt * 1.11, c.maxdt);
+    if (t.step == 0 && t.corr_dt == 0.0) dt = std::min(dt, t.cfl_dt * 0.1);
+    if (t.cfl_dt > 0.0) dt = std::min(dt, t.cfl_dt * c.courant);
+    if (t.corr_dt > 0.0) dt = std::min(dt, t.corr_dt * 0.95);
+    ctx->newdt_i = ctx->newdt_i - 1;
+    const int i = ctx->newdt_i;
+    t.new_dt = (dt < t.dt * 0.95) || (dt > t.dt * 1.10 && i < 0) || (dt == c.maxdt && t.dt < dt && i < 0);
+    if (t.new_dt) {
+        if (dt >= t.dt) ctx->newdt_i = 99;
+        t.dt = dt;
+    }
+    return PF_OK;
+}
+
+// main.f90:20-44
+extern "C" int pf_timestep(pf_ctx *ctx, int *ncorr) {
+    PF_ARG(ctx, "null ctx");
+    PF_TRY(require_matrices(ctx));
+    PF_TRY(pf_vel_imposesym(ctx));
+    PF_TRY(pf_vel_transform(ctx));
+    PF_TRY(pf_vel_nonlinear(ctx));
+    if (ctx->cfg.dt < 0.0) {
+        PF_TRY(pf_vel_maxtstep(ctx));
+        PF_TRY(pf_tim_new_tstep(ctx));
+        if (ctx->tim.new_dt) PF_TRY(pf_vel_matrices_impl(ctx));
+    }
+    PF_TRY(pf_vel_predictor(ctx));
+    ctx->tim.it = 1;
+    int nc = 0, status = PF_OK;
+    while (ctx->tim.it != 0) {
+        PF_TRY(pf_vel_transform(ctx));
+        PF_TRY(pf_vel_nonlinear(ctx));
+        PF_TRY(pf_vel_corrector(ctx));
+        const int s = pf_tim_check_cgce(ctx);
+        if (s != PF_OK) status = s;
+        ++nc;
+    }
+    ctx->tim.t = ctx->tim.t + ctx->tim.dt;
+    ctx->tim.step = ctx->tim.step + 1;
+    if (ncorr) *ncorr = nc;
+    return status;
+}
+
+// newton.f90:740-762 (without the periodic shift and output)
+extern "C" int pf_steporbit(pf_ctx *ctx, int nsteps) {
+    PF_ARG(ctx && nsteps >= 0, "pf_steporbit: bad argument");
+    PF_TRY(require_matrices(ctx));
+    for (int s = 0; s < nsteps; ++s) {
+        PF_TRY(pf_vel_imposesym(ctx));
+        PF_TRY(pf_vel_transform(ctx));
+        PF_TRY(pf_vel_nonlinear(ctx));
+        PF_TRY(pf_vel_predictor(ctx));
+        PF_TRY(pf_vel_transform(ctx));
+        PF_TRY(pf_vel_nonlinear(ctx));
+        PF_TRY(vel_corrector_async(ctx));
+        PF_TRY(pf_vel_imposesym(ctx));
+        ctx->tim.t = ctx->tim.t + ctx->tim.dt;
+        ctx->tim.step = ctx->tim.step + 1;
+    }
+    PF_TRY(read_dterr(ctx));
+    ctx->tim.it = 1;
+    return pf_tim_check_cgce(ctx);
+}
+
+extern "C" int pf_diag_energy(pf_ctx *ctx, double *E) {
+    PF_ARG(ctx && E, "null argument");
+    double e = 0.0, t;
+    for (int i = 0; i < 3; ++i) {
+        PF_TRY(pf_norm_host(ctx, ctx->vel[i].d, &t, nullptr, nullptr));
+        e += t;
+    }
+    *E = e;
+    return PF_OK;
+}
+
+// io.f90:627-639
+extern "C" int pf_diag_friction(pf_ctx *ctx, double *Ub, double *Uc, double *Ufr) {
+    PF_ARG(ctx, "null ctx");
+    const Geo &g = ctx->g;
+    const int N = g.N;
+    std::vector<double2> col(N);
+    PF_CUDA(cudaMemcpy2DAsync(col.data(), sizeof(double2), ctx->vel[2].d, g.Hp * sizeof(double2),
+                              sizeof(double2), N, cudaMemcpyDeviceToHost, ctx->stream));
+    PF_CUDA(cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream));
+    PF_CUDA(cudaStreamSynchronize(ctx->stream));
+    const HostMesh &hm = ctx->hm;
+    double ub = 0.0;
+    for (int n = 0; n < N; ++n) ub += col[n].x * hm.intrdr[n];
+    ub = 0.5 + 2.0 * ub;
+    if (ctx->cfg.const_flux) ub = ctx->hsc->Pr0;
+    double uc = 0.0;
+    for (int j = 0; j <= KL; ++j) uc += col[j].x * hm.dr0[0 * (KL + 1) + j];
+    uc = 1.0 + uc;
+    double uf = 0.0;
+    for (int j = 0; j <= KL; ++j) uf += col[N - 1 - KL + j].x * hm.dr1[1 * (KL + 1) + j];
+    uf = std::sqrt(std::fabs((uf - 2.0) / g.Re));
+    if (Ub) *Ub = ub;
+    if (Uc) *Uc = uc;
+    if (Ufr) *Ufr = uf;
+    return PF_OK;
+}

@@ -1,0 +1,467 @@
+"""Python mirror of the reference's Fortran module API for the timestep path.
+
+One ``Pipe`` holds what the reference keeps in module state for one run
+(parameters, mes_D, var_H, tim_*, vel_*, the LU factor sets).  Method names
+are the reference's routine names (variables.f90, transform.fftw3.f90,
+timestep.f90, velocity.f90) and keep their argument meaning; every non-zero
+status of the C ABI raises ``PipeflowError`` with the library's message --
+the reference's ``stop 'msg'``.
+
+Host arrays use the reference's indexing: a coll component is a pair of
+float64 arrays (re, im) of shape (N, H) indexed [n, nh] (== %Re(n+1, nh));
+a phys field is a float64 array of shape (N, Th, Z) (== %Re(z, t, n+1)).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+
+class PipeflowError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+def _check(status: int) -> int:
+    if status != L.PF_OK:
+        msg = L.load().pf_last_error()
+        raise PipeflowError(status, msg.decode() if msg else "")
+    return status
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(L.DP)
+
+
+@dataclass
+class PipeConfig:
+    """parameters.f90:15-51 as a runtime record."""
+    N: int
+    K: int
+    M: int
+    Mp: int = 1
+    Re: float = 2500.0
+    alpha: float = 1.25
+    dt: float = 0.01
+    implicit: float = 0.51
+    dterr: float = 1e-5
+    courant: float = 0.5
+    maxdt: float = 1e99
+    const_flux: bool = True
+    mirrorsym: bool = False
+    shiftrefl: bool = False
+    shiftrott: bool = False
+    r: np.ndarray | None = None
+    precision: int = L.PF_PREC_FP64
+
+    @property
+    def H(self) -> int:
+        return (2 * self.K - 1) * self.M - (self.K - 1)
+
+    @property
+    def Z(self) -> int:
+        return 3 * self.K
+
+    @property
+    def Th(self) -> int:
+        return 3 * self.M
+
+
+class Coll:
+    """A device `type (coll)` field (variables.f90:37-40)."""
+
+    def __init__(self, pipe: "Pipe", handle=None, owned: bool = True):
+        self.pipe = pipe
+        self.owned = owned
+        if handle is None:
+            h = C.c_void_p()
+            _check(pipe.lib.pf_coll_create(pipe.ctx, C.byref(h)))
+            handle = h
+        self.h = handle
+
+    def upload(self, re: np.ndarray, im: np.ndarray) -> "Coll":
+        N, H = self.pipe.N, self.pipe.H
+        re = np.ascontiguousarray(np.asarray(re, dtype=np.float64).reshape(N, H).T)
+        im = np.ascontiguousarray(np.asarray(im, dtype=np.float64).reshape(N, H).T)
+        _check(self.pipe.lib.pf_coll_upload(self.h, _dp(re), _dp(im)))
+        return self
+
+    def download(self):
+        N, H = self.pipe.N, self.pipe.H
+        re = np.empty((H, N))
+        im = np.empty((H, N))
+        _check(self.pipe.lib.pf_coll_download(self.h, _dp(re), _dp(im)))
+        return np.ascontiguousarray(re.T), np.ascontiguousarray(im.T)
+
+    def __del__(self):
+        try:
+            if self.owned and self.h and self.pipe.ctx:
+                self.pipe.lib.pf_coll_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Phys:
+    """A device `type (phys)` field (variables.f90:42-44)."""
+
+    def __init__(self, pipe: "Pipe", handle=None, owned: bool = True):
+        self.pipe = pipe
+        self.owned = owned
+        if handle is None:
+            h = C.c_void_p()
+            _check(pipe.lib.pf_phys_create(pipe.ctx, C.byref(h)))
+            handle = h
+        self.h = handle
+
+    def upload(self, p: np.ndarray) -> "Phys":
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        assert p.shape == (self.pipe.N, self.pipe.Th, self.pipe.Z)
+        _check(self.pipe.lib.pf_phys_upload(self.h, _dp(p)))
+        return self
+
+    def download(self) -> np.ndarray:
+        out = np.empty((self.pipe.N, self.pipe.Th, self.pipe.Z))
+        _check(self.pipe.lib.pf_phys_download(self.h, _dp(out)))
+        return out
+
+    def __del__(self):
+        try:
+            if self.owned and self.h and self.pipe.ctx:
+                self.pipe.lib.pf_phys_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Mesh:
+    """A set of per-mode `type (mesh)` band matrices (meshs.f90:37-39)."""
+
+    def __init__(self, pipe, h):
+        self.pipe, self.h = pipe, h
+
+    def download(self) -> np.ndarray:
+        """(H, N, 2KL+1) array: [nh, j, row] == A(nh)%M(row+1, j+1)."""
+        out = np.empty((self.pipe.H, self.pipe.N, 2 * L.KL + 1))
+        _check(self.pipe.lib.pf_mesh_download(self.h, _dp(out)))
+        return out
+
+    def __del__(self):
+        try:
+            self.pipe.lib.pf_mesh_destroy(self.h)
+        except Exception:
+            pass
+
+
+class LUMesh:
+    """A set of per-mode `type (lumesh)` LU factors (meshs.f90:42-45)."""
+
+    def __init__(self, pipe, h):
+        self.pipe, self.h = pipe, h
+
+    def download(self):
+        """(M, ipiv): M (H, N, 3KL+1) == A(nh)%M(row+1, j+1); ipiv (H, N) 1-based."""
+        H, N = self.pipe.H, self.pipe.N
+        M = np.empty((H, N, 3 * L.KL + 1))
+        piv = np.empty((H, N), dtype=np.int32)
+        _check(self.pipe.lib.pf_lumesh_download(self.h, _dp(M), piv.ctypes.data_as(L.IP)))
+        return M, piv
+
+    def __del__(self):
+        try:
+            self.pipe.lib.pf_lumesh_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Pipe:
+    """Module state of one pipe on one GPU."""
+
+    def __init__(self, cfg: PipeConfig, device: int = -1):
+        self.lib = L.load()
+        self.cfg = cfg
+        c = L.pf_config()
+        for f in ("N", "K", "M", "Mp", "Re", "alpha", "dt", "implicit", "dterr", "courant", "maxdt"):
+            setattr(c, f, getattr(cfg, f))
+        c.const_flux = int(cfg.const_flux)
+        c.mirrorsym = int(cfg.mirrorsym)
+        c.shiftrefl = int(cfg.shiftrefl)
+        c.shiftrott = int(cfg.shiftrott)
+        c.precision = int(cfg.precision)
+        self._r = None
+        if cfg.r is not None:
+            self._r = np.ascontiguousarray(cfg.r, dtype=np.float64)
+            c.r = _dp(self._r)
+        self.ctx = None
+        h = C.c_void_p()
+        _check(self.lib.pf_ctx_create(C.byref(c), device, C.byref(h)))
+        self.ctx = h
+        N, H, Z, Th = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(self.lib.pf_ctx_dims(self.ctx, C.byref(N), C.byref(H), C.byref(Z), C.byref(Th)))
+        self.N, self.H, self.Z, self.Th = N.value, H.value, Z.value, Th.value
+        self.K, self.M, self.Mp = cfg.K, cfg.M, cfg.Mp
+
+    def close(self):
+        if self.ctx:
+            self.lib.pf_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------- fields ----------------
+    def coll(self, re=None, im=None) -> Coll:
+        c = Coll(self)
+        if re is not None:
+            c.upload(re, im if im is not None else np.zeros_like(re))
+        return c
+
+    def phys(self, p=None) -> Phys:
+        q = Phys(self)
+        if p is not None:
+            q.upload(p)
+        return q
+
+    def vel_field(self, which: int) -> Coll:
+        h = C.c_void_p()
+        _check(self.lib.pf_vel_coll(self.ctx, which, C.byref(h)))
+        return Coll(self, h, owned=False)
+
+    def vel_physfield(self, which: int) -> Phys:
+        h = C.c_void_p()
+        _check(self.lib.pf_vel_phys(self.ctx, which, C.byref(h)))
+        return Phys(self, h, owned=False)
+
+    @property
+    def vel_ur(self):
+        return self.vel_field(0)
+
+    @property
+    def vel_ut(self):
+        return self.vel_field(1)
+
+    @property
+    def vel_uz(self):
+        return self.vel_field(2)
+
+    @property
+    def vel_Nr(self):
+        return self.vel_field(3)
+
+    @property
+    def vel_Nt(self):
+        return self.vel_field(4)
+
+    @property
+    def vel_Nz(self):
+        return self.vel_field(5)
+
+    def set_state(self, ur, ut, uz):
+        """ur, ut, uz: (re, im) pairs of (N, H) arrays."""
+        arrs = []
+        for re, im in (ur, ut, uz):
+            arrs.append(np.ascontiguousarray(np.asarray(re, dtype=np.float64).T))
+            arrs.append(np.ascontiguousarray(np.asarray(im, dtype=np.float64).T))
+        _check(self.lib.pf_vel_set_state(self.ctx, *[_dp(a) for a in arrs]))
+
+    def get_state(self):
+        arrs = [np.empty((self.H, self.N)) for _ in range(6)]
+        _check(self.lib.pf_vel_get_state(self.ctx, *[_dp(a) for a in arrs]))
+        a = [np.ascontiguousarray(x.T) for x in arrs]
+        return [(a[0], a[1]), (a[2], a[3]), (a[4], a[5])]
+
+    def mes_D(self):
+        """Radial mesh: dict of r, dr (KL, N, 2KL+1), radLap (N, 2KL+1), dr0/dr1 (KL+1, KL+1) [i, j], intrdr."""
+        N, KL = self.N, L.KL
+        r = np.empty(N)
+        dr = np.empty((KL, N, 2 * KL + 1))
+        rl = np.empty((N, 2 * KL + 1))
+        d0 = np.empty((KL + 1, KL + 1))
+        d1 = np.empty((KL + 1, KL + 1))
+        w = np.empty(N)
+        _check(self.lib.pf_mes_get(self.ctx, _dp(r), _dp(dr), _dp(rl), _dp(d0), _dp(d1), _dp(w)))
+        return dict(r=r, dr=dr, radLap=rl, dr0=d0, dr1=d1, intrdr=w)
+
+    def sync(self):
+        _check(self.lib.pf_ctx_sync(self.ctx))
+
+    def device_bytes(self) -> int:
+        b = C.c_ulonglong()
+        _check(self.lib.pf_ctx_device_bytes(self.ctx, C.byref(b)))
+        return b.value
+
+    # ---------------- variables.f90 ----------------
+    def var_coll_init(self, a: Coll):
+        _check(self.lib.pf_var_coll_init(a.h))
+
+    def var_coll_copy(self, inp: Coll, out: Coll):
+        _check(self.lib.pf_var_coll_copy(inp.h, out.h))
+
+    def var_coll_add(self, ac: Coll, a: Coll):
+        _check(self.lib.pf_var_coll_add(ac.h, a.h))
+
+    def var_coll_sub(self, ac: Coll, a: Coll):
+        _check(self.lib.pf_var_coll_sub(ac.h, a.h))
+
+    def var_coll_dmult(self, d: float, a: Coll):
+        _check(self.lib.pf_var_coll_dmult(d, a.h))
+
+    def var_coll_neg(self, ac: Coll, a: Coll):
+        _check(self.lib.pf_var_coll_neg(ac.h, a.h))
+
+    def var_coll_meshmult(self, p: int, inp: Coll, out: Coll):
+        _check(self.lib.pf_var_coll_meshmult(p, inp.h, out.h))
+
+    def var_coll_curl(self, r: Coll, t: Coll, z: Coll, o_r: Coll, o_t: Coll, o_z: Coll):
+        _check(self.lib.pf_var_coll_curl(r.h, t.h, z.h, o_r.h, o_t.h, o_z.h))
+
+    def var_coll_grad(self, p: Coll, r: Coll, t: Coll, z: Coll):
+        _check(self.lib.pf_var_coll_grad(p.h, r.h, t.h, z.h))
+
+    def var_coll_div(self, r: Coll, t: Coll, z: Coll, dv: Coll):
+        _check(self.lib.pf_var_coll_div(r.h, t.h, z.h, dv.h))
+
+    def var_coll_shift(self, dt: float, dz: float, a: Coll, b: Coll):
+        _check(self.lib.pf_var_coll_shift(dt, dz, a.h, b.h))
+
+    def var_imposesym(self, i: int, r: Coll, t: Coll, z: Coll):
+        _check(self.lib.pf_var_imposesym(i, r.h, t.h, z.h))
+
+    def var_coll_norm(self, a: Coll):
+        E = C.c_double()
+        Ek = np.empty(self.K)
+        Em = np.empty(self.M)
+        _check(self.lib.pf_var_coll_norm(a.h, C.byref(E), _dp(Ek), _dp(Em)))
+        return E.value, Ek, Em
+
+    # ---------------- transform.fftw3.f90 ----------------
+    def tra_coll2phys(self, c: Coll, p: Phys):
+        _check(self.lib.pf_tra_coll2phys(c.h, p.h))
+
+    def tra_phys2coll(self, p: Phys, c: Coll):
+        _check(self.lib.pf_tra_phys2coll(p.h, c.h))
+
+    tra_spec2phys = tra_coll2phys
+    tra_phys2spec = tra_phys2coll
+
+    # ---------------- timestep.f90 ----------------
+    @property
+    def tim(self) -> L.pf_tim_state:
+        s = L.pf_tim_state()
+        _check(self.lib.pf_tim_get(self.ctx, C.byref(s)))
+        return s
+
+    def set_tim(self, s: L.pf_tim_state):
+        _check(self.lib.pf_tim_set(self.ctx, C.byref(s)))
+
+    def tim_mesh_init(self, PM: int, c1: float, c2: float) -> Mesh:
+        h = C.c_void_p()
+        _check(self.lib.pf_tim_mesh_init(self.ctx, PM, c1, c2, C.byref(h)))
+        return Mesh(self, h)
+
+    def tim_lumesh_init(self, PM: int, BC: int, c1: float, c2: float) -> LUMesh:
+        h = C.c_void_p()
+        _check(self.lib.pf_tim_lumesh_init(self.ctx, PM, BC, c1, c2, C.byref(h)))
+        return LUMesh(self, h)
+
+    def tim_lumesh_invert(self, BC: int, A: LUMesh, b: Coll):
+        _check(self.lib.pf_tim_lumesh_invert(BC, A.h, b.h))
+
+    def tim_meshmult(self, S: int, A: Mesh, b: Coll, c: Coll, d: Coll):
+        _check(self.lib.pf_tim_meshmult(S, A.h, b.h, c.h, d.h))
+
+    def tim_zerobc(self, a: Coll):
+        _check(self.lib.pf_tim_zerobc(a.h))
+
+    def tim_nlincorr(self, N_: Coll, Nn: Coll):
+        _check(self.lib.pf_tim_nlincorr(N_.h, Nn.h))
+
+    def tim_measurecorr(self, c1: Coll, c2: Coll, c3: Coll):
+        _check(self.lib.pf_tim_measurecorr(c1.h, c2.h, c3.h))
+
+    def tim_check_cgce(self):
+        _check(self.lib.pf_tim_check_cgce(self.ctx))
+
+    def tim_new_tstep(self):
+        _check(self.lib.pf_tim_new_tstep(self.ctx))
+
+    # ---------------- velocity.f90 ----------------
+    def vel_imposesym(self):
+        _check(self.lib.pf_vel_imposesym(self.ctx))
+
+    def vel_matrices(self):
+        _check(self.lib.pf_vel_matrices(self.ctx))
+
+    def vel_transform(self):
+        _check(self.lib.pf_vel_transform(self.ctx))
+
+    def vel_nonlinear(self):
+        _check(self.lib.pf_vel_nonlinear(self.ctx))
+
+    def vel_predictor(self):
+        _check(self.lib.pf_vel_predictor(self.ctx))
+
+    def vel_corrector(self):
+        _check(self.lib.pf_vel_corrector(self.ctx))
+
+    def vel_maxtstep(self):
+        _check(self.lib.pf_vel_maxtstep(self.ctx))
+
+    @property
+    def vel_Pr0(self) -> float:
+        p = C.c_double()
+        _check(self.lib.pf_vel_get_scalars(self.ctx, C.byref(p), None))
+        return p.value
+
+    def influence(self):
+        """U (6, H, N) and the inverted A (H, 4, 4) of vel_adjPPE(0)."""
+        U = np.empty((6, self.H, self.N))
+        A = np.empty((self.H, 4, 4))  # memory [nh][j][i] -> transpose below
+        _check(self.lib.pf_vel_influence_download(self.ctx, _dp(U), _dp(A)))
+        return U, np.ascontiguousarray(A.transpose(0, 2, 1))
+
+    # ---------------- drivers ----------------
+    def timestep(self) -> int:
+        n = C.c_int()
+        _check(self.lib.pf_timestep(self.ctx, C.byref(n)))
+        return n.value
+
+    def steporbit(self, nsteps: int):
+        _check(self.lib.pf_steporbit(self.ctx, nsteps))
+
+    def energy(self) -> float:
+        E = C.c_double()
+        _check(self.lib.pf_diag_energy(self.ctx, C.byref(E)))
+        return E.value
+
+    def friction(self):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        _check(self.lib.pf_diag_friction(self.ctx, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    # ---------------- instrumentation ----------------
+    KERNEL_CATEGORIES = ("zinv", "thinv", "thfwd", "zfwd", "lusolve", "stencil", "ew", "infl",
+                         "factor", "step")
+
+    def launches(self) -> int:
+        n = C.c_ulonglong()
+        _check(self.lib.pf_ctx_launches(self.ctx, C.byref(n)))
+        return n.value
+
+    def prof_enable(self, on: bool = True):
+        _check(self.lib.pf_prof_enable(self.ctx, int(on)))
+
+    def prof_read(self):
+        """{category: (total ms, launches)} since prof_enable."""
+        out = {}
+        for i, name in enumerate(self.KERNEL_CATEGORIES):
+            ms, n = C.c_double(), C.c_ulonglong()
+            _check(self.lib.pf_prof_read(self.ctx, i, C.byref(ms), C.byref(n)))
+            out[name] = (ms.value, n.value)
+        return out

@@ -1,0 +1,238 @@
+"""Per-routine parity of the CUDA path (through the C ABI) against the FP64
+oracle on identical seeded inputs.  Tolerances are relative L2 unless noted;
+FP64 routines are held to ~1e-13, i.e. rounding-order differences only."""
+import numpy as np
+import pytest
+
+import pipeflow_oracle as O
+from _util import (CFG1, SMALL, device_pipe, from_dev, oracle_pipe, rand_coll, rel, rel_coll,
+                   state_from_dev, state_to_dev, to_dev)
+
+pytestmark = pytest.mark.gpu
+CASES = SMALL + [CFG1]
+TOL = 1e-13
+
+
+@pytest.fixture(params=range(len(CASES)), ids=lambda i: "N{N}K{K}M{M}Mp{Mp}".format(**CASES[i]))
+def pair(request):
+    cfgd = CASES[request.param]
+    return oracle_pipe(cfgd), device_pipe(cfgd)
+
+
+def test_mesh(pair):
+    o, g = pair
+    m = g.mes_D()
+    D = o.mes_D
+    assert rel(m["r"], D.r) < 1e-15
+    for i in range(O.KL):
+        assert rel(m["dr"][i].T, D.dr[i]) < 1e-11
+    assert rel(m["radLap"].T, D.radLap) < 1e-11
+    assert rel(m["intrdr"], D.intrdr) < 1e-13
+
+
+def test_coll_roundtrip_and_algebra(pair):
+    o, g = pair
+    rng = np.random.default_rng(1)
+    a, b = rand_coll(o.N, o.H, rng), rand_coll(o.N, o.H, rng)
+    da, db = to_dev(g, a), to_dev(g, b)
+    assert rel_coll(from_dev(da), a) == 0.0
+    g.var_coll_add(da, db)
+    assert rel_coll(from_dev(db), O.Coll(a.re + b.re, a.im + b.im)) == 0.0
+    g.var_coll_dmult(0.5, db)
+    assert rel_coll(from_dev(db), O.Coll(0.5 * (a.re + b.re), 0.5 * (a.im + b.im))) == 0.0
+
+
+def test_meshmult_curl_grad_div(pair):
+    o, g = pair
+    rng = np.random.default_rng(2)
+    r, t, z = (rand_coll(o.N, o.H, rng) for _ in range(3))
+    dr, dt, dz = to_dev(g, r), to_dev(g, t), to_dev(g, z)
+    out = [g.coll() for _ in range(3)]
+    for p in range(1, O.KL + 1):
+        g.var_coll_meshmult(p, dr, out[0])
+        assert rel_coll(from_dev(out[0]), o.var_coll_meshmult(o.mes_D.dr[p - 1], r)) < TOL
+    g.var_coll_curl(dr, dt, dz, *out)
+    for got, ref in zip(out, o.var_coll_curl(r, t, z)):
+        assert rel_coll(from_dev(got), ref) < TOL
+    g.var_coll_grad(dr, *out)
+    for got, ref in zip(out, o.var_coll_grad(r)):
+        assert rel_coll(from_dev(got), ref) < TOL
+    g.var_coll_div(dr, dt, dz, out[0])
+    assert rel_coll(from_dev(out[0]), o.var_coll_div(r, t, z)) < TOL
+    # in-place use: curl(u) written over u (copy-in semantics)
+    g.var_coll_curl(dr, dt, dz, dr, dt, dz)
+    for got, ref in zip((dr, dt, dz), o.var_coll_curl(r, t, z)):
+        assert rel_coll(from_dev(got), ref) < TOL
+
+
+def test_transforms(pair):
+    o, g = pair
+    rng = np.random.default_rng(3)
+    c = rand_coll(o.N, o.H, rng)
+    dc = to_dev(g, c)
+    p = g.phys()
+    g.tra_coll2phys(dc, p)
+    ref = o.tra_spec2phys(c)
+    assert rel(p.download(), ref) < TOL
+    phys = rng.standard_normal((o.N, o.cfg.Th, o.cfg.Z))
+    dp = g.phys(phys)
+    out = g.coll()
+    g.tra_phys2coll(dp, out)
+    assert rel_coll(from_dev(out), o.tra_phys2spec(phys)) < TOL
+
+
+def test_lumesh_factor_and_solve(pair):
+    o, g = pair
+    rng = np.random.default_rng(4)
+    for PM, BC, c1, c2 in ((0, 1, 0.0, 1.0), (1, 0, 100.0, -0.51 / 2000), (-1, 0, 50.0, -2e-4),
+                           (0, 0, 100.0, -0.51 / 2000)):
+        ref_AB, ref_piv = o.tim_lumesh_init(PM, BC, c1, c2)
+        A = g.tim_lumesh_init(PM, BC, c1, c2)
+        M, piv = A.download()
+        for nh in range(o.H):
+            if BC == 1 and nh == 0:
+                continue
+            assert np.array_equal(piv[nh] - 1, ref_piv[nh]), (PM, BC, nh)
+            assert rel(M[nh].T, ref_AB[nh]) < 1e-13
+        b = rand_coll(o.N, o.H, rng)
+        db = to_dev(g, b)
+        g.tim_lumesh_invert(BC, A, db)
+        x = b.copy()
+        o.tim_lumesh_invert(BC, (ref_AB, ref_piv), x)
+        assert rel_coll(from_dev(db), x) < 1e-12
+
+
+def test_tim_meshmult(pair):
+    o, g = pair
+    rng = np.random.default_rng(5)
+    b, c = rand_coll(o.N, o.H, rng), rand_coll(o.N, o.H, rng)
+    for PM in (-1, 0, 1):
+        A = g.tim_mesh_init(PM, 100.0, 2.5e-4)
+        ref = o.tim_meshmult(o.tim_mesh_init(PM, 100.0, 2.5e-4), b, c)
+        d = g.coll()
+        g.tim_meshmult(1, A, to_dev(g, b), to_dev(g, c), d)
+        assert rel_coll(from_dev(d), ref) < TOL
+        off, diag = o.tim_mesh_init(PM, 100.0, 2.5e-4)
+        M = A.download()
+        assert rel(M[:, :, O.KL], diag.T) < 1e-15
+
+
+def test_norm_symmetry_shift(pair):
+    o, g = pair
+    rng = np.random.default_rng(6)
+    r, t, z = (rand_coll(o.N, o.H, rng) for _ in range(3))
+    E, Ek, Em = g.var_coll_norm(to_dev(g, r))
+    Er, Ekr, Emr = o.var_coll_norm(r)
+    assert abs(E - Er) < 1e-13 * Er and rel(Ek, Ekr) < 1e-13 and rel(Em, Emr) < 1e-13
+    for i in (0, 1, 2, 3):
+        dr, dt, dz = to_dev(g, r), to_dev(g, t), to_dev(g, z)
+        g.var_imposesym(i, dr, dt, dz)
+        rr, tt, zz = r.copy(), t.copy(), z.copy()
+        o.var_imposesym(i, rr, tt, zz)
+        for got, ref in zip((dr, dt, dz), (rr, tt, zz)):
+            assert rel_coll(from_dev(got), ref) < 1e-15
+    out = g.coll()
+    g.var_coll_shift(0.3, 1.1, to_dev(g, r), out)
+    assert rel_coll(from_dev(out), o.var_coll_shift(0.3, 1.1, r)) < 1e-14
+
+
+def test_influence_matrices(pair):
+    o, g = pair
+    o.vel_matrices()
+    g.vel_matrices()
+    U, A = g.influence()
+    for c in range(6):
+        assert rel(U[c].T, o._U[c]) < 1e-12
+    assert rel(A[1:], o._A[1:]) < 1e-11
+
+
+def test_transform_nonlinear_predictor_corrector(pair):
+    o, g = pair
+    o.vel_matrices()
+    g.vel_matrices()
+    st = O.seeded_state(o, 11, 1e-3)
+    o.set_state(*st)
+    state_to_dev(g, st)
+    o.vel_transform()
+    g.vel_transform()
+    for i, name in enumerate(("r", "t", "z", "curlr", "curlt", "curlz")):
+        assert rel(g.vel_physfield(i).download(), o.phys[name]) < TOL
+    o.vel_nonlinear()
+    g.vel_nonlinear()
+    for i, ref in enumerate((o.vel_Nr, o.vel_Nt, o.vel_Nz)):
+        assert rel_coll(from_dev(g.vel_field(3 + i)), ref) < 1e-12
+    assert abs(g.vel_Pr0 - o.vel_Pr0) <= 1e-12 * max(1.0, abs(o.vel_Pr0))
+    o.vel_predictor()
+    g.vel_predictor()
+    for got, ref in zip(state_from_dev(g), o.state()):
+        assert rel_coll(got, ref) < 1e-12
+    o.vel_transform(); o.vel_nonlinear(); o.vel_corrector()
+    g.vel_transform(); g.vel_nonlinear(); g.vel_corrector()
+    for got, ref in zip(state_from_dev(g), o.state()):
+        assert rel_coll(got, ref) < 1e-12
+    assert abs(g.tim.dterr - o.tim_dterr) <= 1e-9 * o.tim_dterr
+
+
+def test_hagen_poiseuille_preserved_exactly():
+    g = device_pipe(CFG1)
+    g.vel_matrices()
+    for _ in range(3):
+        g.timestep()
+    for re, im in g.get_state():
+        assert np.all(re == 0.0) and np.all(im == 0.0)
+
+
+def test_one_step_parity_cfg1():
+    o, g = oracle_pipe(CFG1), device_pipe(CFG1)
+    o.vel_matrices()
+    g.vel_matrices()
+    st = O.seeded_state(o, 1, 1e-3)
+    o.set_state(*st)
+    state_to_dev(g, st)
+    nco = o.timestep()
+    ncg = g.timestep()
+    assert nco == ncg
+    err = O.rel_l2(state_from_dev(g), o.state())
+    assert err <= 1e-12, err
+
+
+@pytest.mark.slow
+def test_hundred_step_parity_cfg1():
+    o, g = oracle_pipe(CFG1), device_pipe(CFG1)
+    o.vel_matrices()
+    g.vel_matrices()
+    st = O.seeded_state(o, 1, 1e-3)
+    o.set_state(*st)
+    state_to_dev(g, st)
+    for _ in range(100):
+        o.timestep()
+        g.timestep()
+    err = O.rel_l2(state_from_dev(g), o.state())
+    assert err <= 1e-9, err
+    assert abs(g.energy() - o.energy()) <= 1e-9 * o.energy()
+    fr_g, fr_o = g.friction(), o.friction()
+    assert abs(fr_g[2] - fr_o[2]) <= 1e-9 * fr_o[2]
+
+
+def test_noslip_flux_after_steps():
+    g = device_pipe(CFG1)
+    g.vel_matrices()
+    import pipeflow as P
+    P.seeded_state(g, 5, 1e-3)
+    for _ in range(3):
+        g.timestep()
+    st = g.get_state()
+    scale = max(np.abs(re).max() + np.abs(im).max() for re, im in st)
+    for re, im in st:
+        assert np.max(np.abs(re[-1])) < 1e-13 * scale and np.max(np.abs(im[-1])) < 1e-13 * scale
+    intrdr = g.mes_D()["intrdr"]
+    assert abs(2.0 * st[2][0][:, 0] @ intrdr) < 1e-14 * scale
+
+
+def test_device_seeded_state_matches_oracle():
+    import pipeflow as P
+    o, g = oracle_pipe(CFG1), device_pipe(CFG1)
+    P.seeded_state(g, 9, 1e-3)
+    err = O.rel_l2(state_from_dev(g), O.seeded_state(o, 9, 1e-3))
+    assert err < 1e-13
+    assert abs(g.energy() - 1e-3 * np.pi ** 2 / (3 * 1.25)) < 1e-15
