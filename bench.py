@@ -1,0 +1,296 @@
+#!/usr/bin/env python
+"""Timestep throughput of the B200 pipe-flow hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload cfg2|cfg1] [--spinup S]
+
+Workload (default cfg2): the larger plain FP64 drop-in case, N=64 radial
+points, K=128 axial and M=48 azimuthal modes, Mp=2, Re=5300, alpha=0.5,
+dt=0.005, seeded Hagen-Poiseuille + solenoidal perturbation at 0.1 of the
+laminar energy, spun up S (=500) steps before timing.  A "step" is one pass of
+the main.f90 loop body: nonlinear terms, predictor, corrector iterated to
+convergence.  Multi-GPU runs are independent replicas (one pipe per rank,
+seed offset by rank, no collective on the data path); the only collectives
+are the barrier and the max-over-ranks of the timed duration.
+
+--impl reference times the CPU restatement of the reference's step (the FP64
+oracle; the Fortran reference has no compiler on this image) on a bounded
+sample of the same workload, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "softx-d-17-00015_b200"))
+
+METRIC = "batched timesteps/s vs plain at ≤1e-6 rel-L2 vs FP64; serve p50/p99 latency"
+WORKLOADS = {
+    "cfg2": dict(N=64, K=128, M=48, Mp=2, Re=5300.0, alpha=0.5, dt=0.005, energy=0.1, seed=2, spinup=500),
+    "cfg1": dict(N=40, K=24, M=16, Mp=1, Re=2000.0, alpha=1.25, dt=0.01, energy=1e-3, seed=1, spinup=0),
+}
+PHYS = ("N", "K", "M", "Mp", "Re", "alpha", "dt")
+
+
+def coll_bytes(w):
+    H = (2 * w["K"] - 1) * w["M"] - (w["K"] - 1)
+    return w["N"] * H * 16  # one FP64 complex coll field, S
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                      f"--id={self.idx}"], capture_output=True, text=True, timeout=5).stdout
+                for line in out.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_baseline(w, nsteps: int):
+    """Time the FP64 oracle (CPU restatement of the reference step)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pipeflow_oracle as O
+    o = O.Pipe(O.PipeConfig(**{k: w[k] for k in PHYS}))
+    o.vel_matrices()
+    o.set_state(*O.seeded_state(o, w["seed"], w["energy"]))
+    o.timestep()  # untimed warm-up
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        o.timestep()
+    dt = time.perf_counter() - t0
+    return {"value": nsteps / dt, "unit": "timesteps/s", "cores": 1, "kind": "port",
+            "sample": f"{nsteps} steps of the FP64 numpy/scipy oracle on the same workload "
+                      f"(after matrices, seed and 1 warm-up step; no spin-up)"}
+
+
+def run_reference(args, w, rank):
+    if rank != 0:
+        return
+    nsteps = max(1, min(args.steps, args.ref_steps))
+    base = cpu_baseline(w, nsteps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": base["value"], "unit": "timesteps/s",
+        "n_gpus": args.gpus, "steps": nsteps, "warmup": 1, "ms_per_step": 1e3 / base["value"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_of(args, w),
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_of(args, w):
+    H = (2 * w["K"] - 1) * w["M"] - (w["K"] - 1)
+    return {"workload": f"{args.workload}: plain FP64 drop-in, N={w['N']} K={w['K']} M={w['M']} Mp={w['Mp']} "
+                        f"Re={w['Re']} alpha={w['alpha']} dt={w['dt']}, seeded perturbation E={w['energy']} E_lam, "
+                        f"spin-up {w['spinup']} steps",
+            "N": w["N"], "K": w["K"], "M": w["M"], "Mp": w["Mp"], "H": H, "Re": w["Re"], "alpha": w["alpha"],
+            "dt": w["dt"], "pipes_per_gpu": 1, "parallelism": f"replicas x{args.gpus}",
+            "l2": "working set (~0.7 GB) larger than the 126 MB L2; no flush"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg2", choices=list(WORKLOADS))
+    ap.add_argument("--spinup", type=int, default=None)
+    ap.add_argument("--ref-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    w = dict(WORKLOADS[args.workload])
+    if args.spinup is not None:
+        w["spinup"] = args.spinup
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, w, rank)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    import pipeflow as P
+
+    pipe = P.Pipe(P.PipeConfig(**{k: w[k] for k in PHYS}), device=local)
+    stream = torch.cuda.Stream()
+    pipe.lib.pf_ctx_set_stream(pipe.ctx, stream.cuda_stream)
+    pipe.vel_matrices()
+    P.seeded_state(pipe, w["seed"] + rank, w["energy"])
+    with torch.cuda.stream(stream):
+        for _ in range(w["spinup"]):
+            pipe.timestep()
+        # warm-up with every kernel category timed to find the dominant one
+        pipe.prof_enable(True)
+        for _ in range(args.warmup):
+            pipe.timestep()
+        prof = pipe.prof_read()
+        dom = max(prof, key=lambda k: prof[k][0])
+        pipe.prof_enable([dom])
+        stream.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        n0 = pipe.launches()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ncorr = 0
+        with ClockSampler(local) as clk:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                ncorr += pipe.timestep()
+            ev1.record(stream)
+            stream.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        launches = pipe.launches() - n0
+        ms = ev0.elapsed_time(ev1)
+        dom_ms, dom_n = pipe.prof_read()[dom]
+        pipe.prof_enable(False)
+
+        # end to end through the C ABI with pinned host buffers
+        N, H = pipe.N, pipe.H
+        host = [torch.empty((H, N), dtype=torch.float64, pin_memory=True) for _ in range(6)]
+        ptrs = [P.api.C.cast(t.data_ptr(), P._lib.DP) for t in host]
+        P.api._check(pipe.lib.pf_vel_get_state(pipe.ctx, *ptrs))
+        ne = max(1, min(args.e2e_steps, args.steps))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ne):
+            P.api._check(pipe.lib.pf_vel_set_state(pipe.ctx, *ptrs))
+            pipe.timestep()
+            P.api._check(pipe.lib.pf_vel_get_state(pipe.ctx, *ptrs))
+        e1.record(stream)
+        stream.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+
+    if dist:
+        t = torch.tensor([ms, e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    value = world * args.steps / (ms / 1e3)
+    e2e_value = world * ne / (e2e_ms / 1e3)
+
+    if rank == 0:
+        S = coll_bytes(w)
+        peak, src = peaks()
+        # algorithmic bytes of one launch of the dominant category: the coll
+        # fields it must read and write once (factors, twiddles, FFT scratch
+        # are not algorithmic)
+        per_launch = {"lusolve": 2 * S, "stencil": 2 * S, "ew": 2 * S, "infl": 4 * S,
+                      "zinv": 3 * S, "thinv": 3 * S, "thfwd": 3 * S, "zfwd": 3 * S, "step": 12 * S,
+                      "factor": 0}[dom]
+        avg_launch_s = (dom_ms / 1e3) / max(dom_n, 1)
+        achieved = per_launch / avg_launch_s / 1e9 if avg_launch_s > 0 else None
+        traffic = read_traffic(dom, args.workload)
+        line = {
+            "metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_of(args, w),
+            "corrector_iterations_per_step": ncorr / args.steps,
+            "algorithmic_bytes_per_step": S * (15 + 21 * ncorr / args.steps),
+            "step_bandwidth_gbs": S * (15 + 21 * ncorr / args.steps) / (ms / args.steps / 1e3) / 1e9,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "peak_source": src, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None,
+                         "algorithmic_bytes_per_launch": per_launch,
+                         "avg_launch_us": avg_launch_s * 1e6, "launches": dom_n,
+                         "traffic": traffic},
+            "gpu_launches": launches,
+            "e2e": {"value": e2e_value, "unit": "timesteps/s", "steps": ne,
+                    "h2d_bytes_per_step": 6 * N * H * 8, "d2h_bytes_per_step": 6 * N * H * 8},
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(w, max(1, args.ref_steps))
+        print(json.dumps(line), flush=True)
+    pipe.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def read_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == workload and parts[1] == kernel:
+            try:
+                return float(parts[2])
+            except ValueError:
+                return None
+    return None
+
+
+if __name__ == "__main__":
+    main()

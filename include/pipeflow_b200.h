@@ -219,8 +219,9 @@ int pf_diag_friction(pf_ctx *ctx, double *Ub, double *Uc, double *Ufr);
 #define PF_K_NCAT    10
 /* Count of this library's kernel launches on the context since creation. */
 int pf_ctx_launches(const pf_ctx *ctx, unsigned long long *n);
-/* Enable (1) / disable (0) per-category event timing; enabling clears totals. */
-int pf_prof_enable(pf_ctx *ctx, int on);
+/* Event timing for the categories whose bit (1 << PF_K_*) is set in mask;
+ * 0 disables.  Each call clears the totals. */
+int pf_prof_enable(pf_ctx *ctx, int mask);
 /* Total device milliseconds and launches of category `cat` since enabling
  * (synchronises the stream). */
 int pf_prof_read(pf_ctx *ctx, int cat, double *ms, unsigned long long *launches);

@@ -154,6 +154,8 @@ static int ctx_init(pf_ctx *ctx, const pf_config *cfg, int device) {
     PF_TRY(pf_alloc(ctx, (void **)&ctx->Ainv, (size_t)16 * g.Hp * sizeof(double)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->Ui, (size_t)N * sizeof(double)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->red, (size_t)(3 * N + g.Hp + 64) * sizeof(double)));
+    PF_TRY(pf_alloc(ctx, (void **)&ctx->cflmax, (size_t)3 * N * sizeof(unsigned long long)));
+    PF_TRY(pf_alloc(ctx, (void **)&ctx->anypiv, sizeof(int)));
     ctx->T_bytes = (size_t)6 * N * g.M * g.Z * sizeof(double2);
     PF_TRY(pf_alloc(ctx, &ctx->T, ctx->T_bytes));
     // LU factor storage for the four matrix sets
@@ -520,14 +522,14 @@ extern "C" int pf_ctx_launches(const pf_ctx *ctx, unsigned long long *n) {
     return PF_OK;
 }
 
-extern "C" int pf_prof_enable(pf_ctx *ctx, int on) {
+extern "C" int pf_prof_enable(pf_ctx *ctx, int mask) {
     PF_ARG(ctx, "null ctx");
     prof_drain(ctx);
     for (int c = 0; c < PF_K_NCAT; ++c) {
         ctx->prof_ms[c] = 0.0;
         ctx->prof_n[c] = 0;
     }
-    ctx->prof_on = on != 0;
+    ctx->prof_mask = mask;
     return PF_OK;
 }
 

@@ -373,14 +373,22 @@ __global__ void k_maxphys(const double *__restrict__ pr, const double *__restric
 
 int pf_launch_maxtstep(pf_ctx *ctx, double *dt3) {
     const Geo &g = ctx->g;
+    std::vector<double> mx(3 * g.N);
+    if (ctx->cfl_fused) {  // maxima left by the fused theta pass
+        std::vector<unsigned long long> bits(3 * g.N);
+        PF_CUDA(cudaMemcpyAsync(bits.data(), ctx->cflmax, bits.size() * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+        PF_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (int i = 0; i < 3 * g.N; ++i) mx[i] = bits_to_double(bits[i]);
+    } else {
     {
         ProfScope ps_(ctx, PF_K_EW);
         k_maxphys<<<g.N, 256, 0, ctx->stream>>>(ctx->phys[0].d, ctx->phys[1].d, ctx->phys[2].d, ctx->red, ctx->dm, g);
     }
     PF_LAUNCHED(ctx);
-    std::vector<double> mx(3 * g.N);
     PF_CUDA(cudaMemcpyAsync(mx.data(), ctx->red, mx.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     PF_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
     const double PI = 3.1415926535897931;
     const std::vector<double> &r = ctx->hm.r;
     const int N = g.N;

@@ -121,6 +121,7 @@ struct pf_mesh {
 struct pf_lumesh {
     pf_ctx *ctx;
     int PM, BC;
+    int pivoted;         // host copy: any row interchange in the factorisation
     double c1, c2;
     double *lu;
     unsigned char *piv;
@@ -159,13 +160,16 @@ struct pf_ctx {
     double *Ainv;        // inverted 4x4 [(i*4+j)*Hp + nh] == A(i+1,j+1,nh)
     double *Ui;          // flux influence vector [N]
     double *red;         // reduction scratch (>= 3*N + H doubles)
+    unsigned long long *cflmax;  // 3*N CFL maxima of the last fused transform
+    bool cfl_fused;              // cflmax is current (else use vel_r/t/z)
+    int *anypiv;         // per LU set: 1 if dgbtf2 swapped any row
     void *T;             // FFT scratch: 6*N*M*Z complex (FP64)
     size_t T_bytes;
     int zinv_mc, zfwd_mc, th_zc;   // tile sizes
     std::vector<void *> allocs;    // everything to free
     // instrumentation
     unsigned long long launches;
-    bool prof_on;
+    int prof_mask;
     std::vector<cudaEvent_t> ev_pool;                 // free events
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_open[PF_K_NCAT];
     double prof_ms[PF_K_NCAT];
@@ -180,7 +184,7 @@ struct ProfScope {
     int cat;
     cudaEvent_t a;
     ProfScope(pf_ctx *c, int k) : ctx(c), cat(k), a(nullptr) {
-        if (ctx->prof_on) {
+        if (ctx->prof_mask & (1 << k)) {
             a = pf_event_get(ctx);
             cudaEventRecord(a, ctx->stream);
         }
@@ -245,3 +249,6 @@ int pf_launch_phys2coll(pf_ctx *ctx, int ncomp, const double *const *src,
                         double2 *const *dst, bool cross);
 int pf_launch_maxtstep(pf_ctx *ctx, double *dt3);
 int pf_norm_host(pf_ctx *ctx, const double2 *a, double *E, double *Ek, double *Em);
+bool pf_nl_fused_supported(const pf_ctx *ctx);
+int pf_launch_nl_fused(pf_ctx *ctx);
+int pf_vel_step_fused(pf_ctx *ctx, int corrector);

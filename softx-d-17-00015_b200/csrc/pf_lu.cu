@@ -15,7 +15,7 @@
 // Assemble A = c1 I + c2 Lap(PM) with the axis-parity first row and the wall
 // row, then factor in place (timestep.f90:75-93; dgbtf2).
 __global__ void k_lu_factor(double *__restrict__ lu, unsigned char *__restrict__ piv, DevMesh dm, Geo g,
-                            int PM, int BC, double c1, double c2, int *info) {
+                            int PM, int BC, double c1, double c2, int *info, int *anypiv) {
     const int nh = blockIdx.x * blockDim.x + threadIdx.x;
     if (nh >= g.H) return;
     const int N = g.N, Hp = g.Hp;
@@ -47,6 +47,7 @@ __global__ void k_lu_factor(double *__restrict__ lu, unsigned char *__restrict__
             }
         }
         piv[(size_t)j * Hp + nh] = (unsigned char)jp;
+        if (jp != 0) atomicOr(anypiv, 1);
         if (LU(KV + jp, j) != 0.0) {
             ju = max(ju, min(j + KL + jp, N - 1));
             if (jp != 0)
@@ -135,14 +136,16 @@ __global__ void k_lu_solve(const double *__restrict__ lu, const unsigned char *_
 int pf_launch_lu_factor(pf_ctx *ctx, pf_lumesh *A) {
     const Geo &g = ctx->g;
     PF_CUDA(cudaMemsetAsync(&ctx->dsc->info, 0, sizeof(int), ctx->stream));
+    PF_CUDA(cudaMemsetAsync(ctx->anypiv, 0, sizeof(int), ctx->stream));
     {
         ProfScope ps_(ctx, PF_K_FACTOR);
         k_lu_factor<<<grid1(g.H, 64), 64, 0, ctx->stream>>>(A->lu, A->piv, ctx->dm, g, A->PM, A->BC, A->c1, A->c2,
-                                                             &ctx->dsc->info);
+                                                             &ctx->dsc->info, ctx->anypiv);
     }
     PF_LAUNCHED(ctx);
     int info = 0;
     PF_CUDA(cudaMemcpyAsync(&info, &ctx->dsc->info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    PF_CUDA(cudaMemcpyAsync(&A->pivoted, ctx->anypiv, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     PF_CUDA(cudaStreamSynchronize(ctx->stream));
     if (info != 0) {
         pf_set_error("tim_lumesh_init: zero pivot in column %d", info);

@@ -36,6 +36,7 @@ extern "C" int pf_vel_transform(pf_ctx *ctx) {
     const double2 *src[6] = {ctx->vel[0].d, ctx->vel[1].d, ctx->vel[2].d, ctx->s[0].d, ctx->s[1].d, ctx->s[2].d};
     double *dst[6];
     for (int i = 0; i < 6; ++i) dst[i] = ctx->phys[i].d;
+    ctx->cfl_fused = false;
     return pf_launch_coll2phys(ctx, 6, src, dst);
 }
 
@@ -85,9 +86,15 @@ static int vel_step(pf_ctx *ctx) {
     return pf_launch_zero_mode0(ctx);
 }
 
+static bool fused_step_ok(const pf_ctx *ctx) {
+    return ctx->g.N <= 128 && !ctx->LDp.pivoted && !ctx->LDm.pivoted && !ctx->LDz.pivoted;
+}
+
 // velocity.f90:400-410
 extern "C" int pf_vel_predictor(pf_ctx *ctx) {
     PF_ARG(ctx, "null ctx");
+    PF_TRY(require_matrices(ctx));
+    if (fused_step_ok(ctx)) return pf_vel_step_fused(ctx, 0);
     for (int i = 0; i < 6; ++i)
         PF_TRY(pf_launch_ew(ctx, EW_COPY, ctx->vel[i].d, nullptr, ctx->prev[i].d, nullptr, 0.0));
     return vel_step(ctx);
@@ -95,6 +102,8 @@ extern "C" int pf_vel_predictor(pf_ctx *ctx) {
 
 // velocity.f90:416-432 (tim_measurecorr folded into one device reduction)
 static int vel_corrector_async(pf_ctx *ctx) {
+    PF_TRY(require_matrices(ctx));
+    if (fused_step_ok(ctx)) return pf_vel_step_fused(ctx, 1);
     for (int i = 0; i < 3; ++i)
         PF_TRY(pf_launch_ew(ctx, EW_COPY, ctx->vel[i].d, nullptr, ctx->save[i].d, nullptr, 0.0));
     for (int i = 3; i < 6; ++i)
@@ -117,6 +126,18 @@ extern "C" int pf_vel_corrector(pf_ctx *ctx) {
     PF_ARG(ctx, "null ctx");
     PF_TRY(vel_corrector_async(ctx));
     return read_dterr(ctx);
+}
+
+// vel_transform + vel_nonlinear for the drivers: the fused three-launch
+// path when the transform lengths are instantiated, else the materialising one
+static int transform_nonlinear(pf_ctx *ctx) {
+    if (pf_nl_fused_supported(ctx)) {
+        PF_TRY(pf_launch_nl_fused(ctx));
+        ctx->cfl_fused = true;
+        return PF_OK;
+    }
+    PF_TRY(pf_vel_transform(ctx));
+    return pf_vel_nonlinear(ctx);
 }
 
 extern "C" int pf_vel_maxtstep(pf_ctx *ctx) {
@@ -191,8 +212,7 @@ extern "C" int pf_timestep(pf_ctx *ctx, int *ncorr) {
     PF_ARG(ctx, "null ctx");
     PF_TRY(require_matrices(ctx));
     PF_TRY(pf_vel_imposesym(ctx));
-    PF_TRY(pf_vel_transform(ctx));
-    PF_TRY(pf_vel_nonlinear(ctx));
+    PF_TRY(transform_nonlinear(ctx));
     if (ctx->cfg.dt < 0.0) {
         PF_TRY(pf_vel_maxtstep(ctx));
         PF_TRY(pf_tim_new_tstep(ctx));
@@ -202,8 +222,7 @@ extern "C" int pf_timestep(pf_ctx *ctx, int *ncorr) {
     ctx->tim.it = 1;
     int nc = 0, status = PF_OK;
     while (ctx->tim.it != 0) {
-        PF_TRY(pf_vel_transform(ctx));
-        PF_TRY(pf_vel_nonlinear(ctx));
+        PF_TRY(transform_nonlinear(ctx));
         PF_TRY(pf_vel_corrector(ctx));
         const int s = pf_tim_check_cgce(ctx);
         if (s != PF_OK) status = s;
@@ -221,11 +240,9 @@ extern "C" int pf_steporbit(pf_ctx *ctx, int nsteps) {
     PF_TRY(require_matrices(ctx));
     for (int s = 0; s < nsteps; ++s) {
         PF_TRY(pf_vel_imposesym(ctx));
-        PF_TRY(pf_vel_transform(ctx));
-        PF_TRY(pf_vel_nonlinear(ctx));
+        PF_TRY(transform_nonlinear(ctx));
         PF_TRY(pf_vel_predictor(ctx));
-        PF_TRY(pf_vel_transform(ctx));
-        PF_TRY(pf_vel_nonlinear(ctx));
+        PF_TRY(transform_nonlinear(ctx));
         PF_TRY(vel_corrector_async(ctx));
         PF_TRY(pf_vel_imposesym(ctx));
         ctx->tim.t = ctx->tim.t + ctx->tim.dt;

@@ -454,8 +454,17 @@ class Pipe:
         _check(self.lib.pf_ctx_launches(self.ctx, C.byref(n)))
         return n.value
 
-    def prof_enable(self, on: bool = True):
-        _check(self.lib.pf_prof_enable(self.ctx, int(on)))
+    def prof_enable(self, on=True):
+        """on: True (all categories), False, or a list of category names."""
+        if on is True:
+            mask = (1 << len(self.KERNEL_CATEGORIES)) - 1
+        elif not on:
+            mask = 0
+        else:
+            mask = 0
+            for name in on:
+                mask |= 1 << self.KERNEL_CATEGORIES.index(name)
+        _check(self.lib.pf_prof_enable(self.ctx, mask))
 
     def prof_read(self):
         """{category: (total ms, launches)} since prof_enable."""
