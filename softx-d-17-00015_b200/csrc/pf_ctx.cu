@@ -156,6 +156,7 @@ static int ctx_init(pf_ctx *ctx, const pf_config *cfg, int device) {
     PF_TRY(pf_alloc(ctx, (void **)&ctx->red, (size_t)(3 * N + g.Hp + 64) * sizeof(double)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->cflmax, (size_t)3 * N * sizeof(unsigned long long)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->anypiv, sizeof(int)));
+    PF_TRY(pf_alloc(ctx, (void **)&ctx->LNp_pivd, (size_t)N * g.Hp * sizeof(double)));
     ctx->T_bytes = (size_t)6 * N * g.M * g.Z * sizeof(double2);
     PF_TRY(pf_alloc(ctx, &ctx->T, ctx->T_bytes));
     // LU factor storage for the four matrix sets

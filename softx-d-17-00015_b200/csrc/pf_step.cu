@@ -1,4 +1,4 @@
-// Fused vel_step (velocity.f90:367-394) in four launches:
+// Fused vel_step (velocity.f90:367-394) in five launches:
 //   S1 k_step_rhs  : tile of 32 modes x all radial points: optional
 //                    nlincorr (timestep.f90:174-184) or N_ := N copy,
 //                    rhs = Lt u_ + N in the u+-/uz variables (velocity.f90:369-373,
@@ -7,17 +7,16 @@
 //                    boundary rows (velocity.f90:228-230)
 //   S2 k_solve_pnp : pressure Poisson solve with LNp (pivoting band LU,
 //                    BC=1, mean mode zeroed; timestep.f90:102-123)
+//   S3 k_step_proj : the projection rhs - rt2pm(grad p) with zero boundary
+//                    rows (velocity.f90:232-236, 376-378)
 //   S4 k_solve_ld  : the u+, u-, uz Helmholtz solves (LDp, LDm, LDz, which
-//                    never pivot); the projection rhs - rt2pm(grad p) with
-//                    zero boundary rows (velocity.f90:232-236, 376-378) is
-//                    formed in the solve's load stage
+//                    never pivot)
 //   S5 k_step_final: influence-matrix correction (velocity.f90:238-256),
 //                    pm2rt, constant-flux adjustment for k=m=0
 //                    (velocity.f90:170-175), mean-mode symmetry zeros, and the
 //                    corrector error max |u_old - u_new|^2 (timestep.f90:190-207)
-// Scratch: v (3 coll) holds rhs then the solutions, p (1 coll) the pressure.
-// One thread per (mode, part) or (mode, system, part) runs each banded
-// solve; the factor columns of the next two steps are loaded ahead.
+// Scratch: v (3 coll) holds rhs then the solutions, prhs/p the pressure
+// right-hand side and solution, rl (3 coll) the Helmholtz right-hand sides.
 #include <cmath>
 #include "pf_internal.cuh"
 
@@ -29,10 +28,12 @@ struct StepArgs {
     double2 *Nl[3];        // vel_N (read; rewritten by nlincorr)
     double2 *N_[3];        // saved N_ (read in the corrector, written in the predictor)
     double2 *v[3];         // scratch: rhs / solutions in u+, u-, uz
+    double2 *prhs;         // scratch: pressure right-hand side
     double2 *p;            // scratch: pressure
+    double2 *rl[3];        // scratch: Helmholtz right-hand sides
     double2 *u[3];         // vel_u (read as u_old by the corrector, written)
     const double *lnp, *ldp, *ldm, *ldz;
-    const unsigned char *pivp;
+    const double *pivd;    // LNp pivots as doubles [col*Hp + nh]
     const double *U, *Ainv, *Ui;
     DevMesh dm;
     Geo g;
@@ -135,46 +136,69 @@ __global__ void __launch_bounds__(TM *TR) k_step_rhs(StepArgs a) {
             dv.x = r.x * rm1 + dr.x - t.y * m1r1 - z.y * kal;   // variables.f90:472-477
             dv.y = r.y * rm1 + dr.y + t.x * m1r1 + z.x * kal;
         }
-        a.p[(size_t)n * Hp + nh] = dv;
+        a.prhs[(size_t)n * Hp + nh] = dv;
     }
 }
 
 // --------------------------------------------------- banded solves (S2, S4)
-// Forward sweep of dgbtrs with the next two factor columns in flight, then
-// the dtbsv back substitution.  PIV selects the pivoting layout (U with
-// KL+KU superdiagonals) or the pivot-free one (KU superdiagonals).
-template <bool PIV, typename Rhs>
-__device__ __forceinline__ void solve_chain(const double *__restrict__ lu, const unsigned char *__restrict__ piv,
-                                            int N, int Hp, int nh, const Rhs &rhs, double *out, size_t ostride) {
+// One thread per (mode, system, re/im) chain.  The factor values of a
+// column and the right-hand side entering the elimination window are staged
+// D columns ahead into a per-thread shared-memory ring with cp.async (8-byte
+// copies, one commit group per column), so each step of the sequential
+// sweep reads shared memory instead of waiting on DRAM.  The ring is laid out
+// [slot][value][thread] so consecutive threads hit consecutive banks.
+static constexpr int RING = 8;
+
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// dgbtrs ('N', one right-hand side) followed by dtbsv: rhs(n) = rhs[n*rs],
+// solution to out[n*os] (out must not alias rhs).  PIV: LAPACK band with
+// KL+KU superdiagonals in U and pivots pivd[col*Hp+nh] (as doubles); else
+// the pivot-free band with KU = KL.
+template <bool PIV>
+__device__ __forceinline__ void solve_async(const double *__restrict__ lu, const double *__restrict__ pivd, int N,
+                                            int Hp, int nh, const double *__restrict__ rhs, size_t rs, double *out,
+                                            size_t os, double *ring, int ts) {
     constexpr int KU = PIV ? KV : KL;
-#define LUQ(row, col) lu[((size_t)(row) * N + (col)) * Hp + nh]
+    constexpr int SWF = KL + 1 + (PIV ? 1 : 0);  // forward slot: L column, rhs ahead, pivot
+    constexpr int SWB = KU + 1;                  // backward slot: U column
+    constexpr int SW = SWF > SWB ? SWF : SWB;
+#define LUA(row, col) (lu + ((size_t)(row) * N + (col)) * Hp + nh)
+#define RSLOT(s, q) ring[((s) * SW + (q)) * ts]
+    auto issue_fwd = [&](int j) {
+        if (j < N) {
+            const int s = j % RING;
+            if (j < N - 1) {
+#pragma unroll
+                for (int i = 0; i < KL; ++i) cp_async8(&RSLOT(s, i), LUA(KV + 1 + i, j));
+                if (PIV) cp_async8(&RSLOT(s, KL + 1), pivd + (size_t)j * Hp + nh);
+            }
+            if (j + KL + 1 < N) cp_async8(&RSLOT(s, KL), rhs + (size_t)(j + KL + 1) * rs);
+        }
+        cp_async_commit();
+    };
     double w[KL + 1];
 #pragma unroll
-    for (int i = 0; i <= KL; ++i) w[i] = rhs(i);
-    double Lc[KL], Ln[KL];
-    int pc = 0, pn = 0;
+    for (int i = 0; i <= KL; ++i) w[i] = (i < N) ? rhs[(size_t)i * rs] : 0.0;
 #pragma unroll
-    for (int i = 0; i < KL; ++i) {
-        Lc[i] = LUQ(KV + 1 + i, 0);
-        Ln[i] = (N > 1) ? LUQ(KV + 1 + i, 1) : 0.0;
-    }
-    if (PIV) {
-        pc = piv[nh];
-        pn = (N > 1) ? piv[(size_t)Hp + nh] : 0;
-    }
+    for (int j = 0; j < RING; ++j) issue_fwd(j);
     for (int j = 0; j < N; ++j) {
-        double Lf[KL];
-        int pf = 0;
-        const bool more = j + 2 < N - 1;
-#pragma unroll
-        for (int i = 0; i < KL; ++i) Lf[i] = more ? LUQ(KV + 1 + i, j + 2) : 0.0;
-        if (PIV && more) pf = piv[(size_t)(j + 2) * Hp + nh];
-        const double ahead = (j + KL + 1 < N) ? rhs(j + KL + 1) : 0.0;
+        cp_async_wait<RING - 1>();
+        const int s = j % RING;
+        const double ahead = (j + KL + 1 < N) ? RSLOT(s, KL) : 0.0;
         if (j < N - 1) {
             if (PIV) {
+                const int p = (int)RSLOT(s, KL + 1);
 #pragma unroll
                 for (int i = 1; i <= KL; ++i)
-                    if (pc == i) {
+                    if (p == i) {
                         const double t = w[0];
                         w[0] = w[i];
                         w[i] = t;
@@ -183,121 +207,131 @@ __device__ __forceinline__ void solve_chain(const double *__restrict__ lu, const
             const double bj = w[0];
 #pragma unroll
             for (int i = 1; i <= KL; ++i)
-                if (j + i < N) w[i] = fma(-Lc[i - 1], bj, w[i]);
+                if (j + i < N) w[i] = fma(-RSLOT(s, i - 1), bj, w[i]);
         }
-        out[(size_t)j * ostride] = w[0];
+        out[(size_t)j * os] = w[0];
 #pragma unroll
         for (int i = 0; i < KL; ++i) w[i] = w[i + 1];
         w[KL] = ahead;
-#pragma unroll
-        for (int i = 0; i < KL; ++i) {
-            Lc[i] = Ln[i];
-            Ln[i] = Lf[i];
-        }
-        pc = pn;
-        pn = pf;
+        issue_fwd(j + RING);
     }
-    // back substitution (dtbsv 'U','N','N' with K = KU superdiagonals)
+    cp_async_wait<0>();
+    // back substitution; y (this thread's forward output) is read through a
+    // four-deep register queue
+    auto issue_bwd = [&](int t) {  // step t handles column N-1-t
+        const int j = N - 1 - t;
+        if (j >= 0) {
+            const int s = t % RING;
+#pragma unroll
+            for (int i = 0; i <= KU; ++i) cp_async8(&RSLOT(s, i), LUA(KV - i, j));
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int t = 0; t < RING; ++t) issue_bwd(t);
     double v[KU + 1];
 #pragma unroll
-    for (int i = 0; i <= KU; ++i) v[i] = (N - 1 - i >= 0) ? out[(size_t)(N - 1 - i) * ostride] : 0.0;
-    double Uc[KU + 1], Un[KU + 1];
+    for (int i = 0; i <= KU; ++i) v[i] = (N - 1 - i >= 0) ? out[(size_t)(N - 1 - i) * os] : 0.0;
+    constexpr int QY = 4;
+    double yq[QY];
 #pragma unroll
-    for (int i = 0; i <= KU; ++i) {
-        Uc[i] = LUQ(KV - i, N - 1);
-        Un[i] = (N > 1) ? LUQ(KV - i, N - 2) : 0.0;
+    for (int q = 0; q < QY; ++q) {
+        const int r = N - 1 - KU - 1 - q;
+        yq[q] = (r >= 0) ? out[(size_t)r * os] : 0.0;
     }
-    for (int j = N - 1; j >= 0; --j) {
-        double Uf[KU + 1];
+    for (int t = 0; t < N; ++t) {
+        const int j = N - 1 - t;
+        cp_async_wait<RING - 1>();
+        const int s = t % RING;
+        const double ahead = yq[0];
 #pragma unroll
-        for (int i = 0; i <= KU; ++i) Uf[i] = (j - 2 >= 0) ? LUQ(KV - i, j - 2) : 0.0;
-        const double ahead = (j - KU - 1 >= 0) ? out[(size_t)(j - KU - 1) * ostride] : 0.0;
+        for (int q = 0; q < QY - 1; ++q) yq[q] = yq[q + 1];
+        {
+            const int r = j - KU - 1 - QY;
+            yq[QY - 1] = (r >= 0) ? out[(size_t)r * os] : 0.0;
+        }
         double x = v[0];
         if (x != 0.0) {
-            x = x / Uc[0];
+            x = x / RSLOT(s, 0);
 #pragma unroll
             for (int i = 1; i <= KU; ++i)
-                if (j - i >= 0) v[i] = fma(-x, Uc[i], v[i]);
+                if (j - i >= 0) v[i] = fma(-x, RSLOT(s, i), v[i]);
         }
-        out[(size_t)j * ostride] = x;
+        out[(size_t)j * os] = x;
 #pragma unroll
         for (int i = 0; i < KU; ++i) v[i] = v[i + 1];
-        v[KU] = ahead;
-#pragma unroll
-        for (int i = 0; i <= KU; ++i) {
-            Uc[i] = Un[i];
-            Un[i] = Uf[i];
-        }
+        v[KU] = (j - KU - 1 >= 0) ? ahead : 0.0;
+        issue_bwd(t + RING);
     }
-#undef LUQ
+    cp_async_wait<0>();
+#undef LUA
+#undef RSLOT
 }
 
-struct RhsPlain {
-    const double *b;
-    size_t stride;
-    __device__ __forceinline__ double operator()(int n) const { return b[(size_t)n * stride]; }
-};
-
-// S2: thread = (mode, re/im)
-__global__ void k_solve_pnp(StepArgs a) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nh = t >> 1, part = t & 1;
+// S2: warp = (re or im) of 32 consecutive modes
+__global__ void __launch_bounds__(64) k_solve_pnp(StepArgs a) {
+    extern __shared__ double ring2[];
     const Geo &g = a.g;
-    if (nh >= g.H) return;
-    double *bp = reinterpret_cast<double *>(a.p) + 2 * (size_t)nh + part;
-    const size_t stride = 2 * (size_t)g.Hp;
+    const int part = threadIdx.x >> 5;
+    const int nh = blockIdx.x * 32 + (threadIdx.x & 31);
+    const bool live = nh < g.H;
+    const size_t st = 2 * (size_t)g.Hp;
+    double *out = reinterpret_cast<double *>(a.p) + 2 * (size_t)nh + part;
+    const double *rhs = reinterpret_cast<const double *>(a.prhs) + 2 * (size_t)nh + part;
+    if (!live) return;
     if (nh == 0) {  // BC=1 at k=m=0: zero (timestep.f90:110-113)
-        for (int n = 0; n < g.N; ++n) bp[n * stride] = 0.0;
+        for (int n = 0; n < g.N; ++n) out[n * st] = 0.0;
         return;
     }
-    solve_chain<true>(a.lnp, a.pivp, g.N, g.Hp, nh, RhsPlain{bp, stride}, bp, stride);
+    solve_async<true>(a.lnp, a.pivd, g.N, g.Hp, nh, rhs, st, out, st, ring2 + threadIdx.x, blockDim.x);
 }
 
-// S4 rhs: v - rt2pm(grad p) (or v_z - i alpha k p), zero at n=0 and n=N-1
-struct RhsProj {
-    const double2 *v, *p;
-    const double *dr, *rm1;
-    int N, Hp, nh, sys, part;
-    double m1, kal;  // m*Mp, alpha*k
-    __device__ __forceinline__ double operator()(int n) const {
-        if (n == 0 || n == N - 1) return 0.0;
-        const size_t at = (size_t)n * Hp + nh;
-        const double2 pv = p[at];
-        const double2 vv = v[at];
-        if (sys == 2) {  // uz: g = (-alpha k p.im, alpha k p.re)
-            return part == 0 ? vv.x - (-pv.y * kal) : vv.y - (pv.x * kal);
-        }
-        double2 dr2 = make_double2(0, 0);
-        const int lo = max(0, n - KL), hi = min(N - 1, n + KL);
-        for (int j = lo; j <= hi; ++j) {
-            const double w = dr[(KL + n - j) * N + j];
-            const double2 x = p[(size_t)j * Hp + nh];
-            dr2.x = fma(w, x.x, dr2.x);
-            dr2.y = fma(w, x.y, dr2.y);
-        }
-        const double m1r1 = rm1[n] * m1;
-        // grad: r = dr p, t = (-p.im m/r, p.re m/r); rt2pm(r, t)
-        const double tRe = -pv.y * m1r1, tIm = pv.x * m1r1;
-        if (sys == 0) return part == 0 ? vv.x - (dr2.x - tIm) : vv.y - (dr2.y + tRe);
-        return part == 0 ? vv.x - (dr2.x + tIm) : vv.y - (dr2.y - tRe);
+// S3: rhs - rt2pm(grad p) (velocity.f90:232-236) with zero boundary rows
+// (velocity.f90:376-378), one thread per (n, mode)
+__global__ void k_step_proj(StepArgs a) {
+    const Geo &g = a.g;
+    const int nh = blockIdx.x * blockDim.x + threadIdx.x, n = blockIdx.y;
+    if (nh >= g.H) return;
+    const size_t at = (size_t)n * g.Hp + nh;
+    if (n == 0 || n == g.N - 1) {
+        a.rl[0][at] = a.rl[1][at] = a.rl[2][at] = make_double2(0.0, 0.0);
+        return;
     }
-};
+    int k, m;
+    mode_km(nh, g.K, k, m);
+    const int N = g.N;
+    double2 dr2 = make_double2(0, 0);
+    const int lo = max(0, n - KL), hi = min(N - 1, n + KL);
+    for (int j = lo; j <= hi; ++j) {
+        const double w = a.dm.dr[(KL + n - j) * N + j];
+        const double2 x = a.p[(size_t)j * g.Hp + nh];
+        dr2.x = fma(w, x.x, dr2.x);
+        dr2.y = fma(w, x.y, dr2.y);
+    }
+    const double2 pv = a.p[at];
+    const double m1r1 = a.dm.rp[2 * N + n] * g.Mp * m;
+    const double kal = g.alpha * k;
+    // grad p = (dr p, i m/r p, i alpha k p); rt2pm of its (r, theta) parts
+    const double tRe = -pv.y * m1r1, tIm = pv.x * m1r1;
+    const double2 vp = a.v[0][at], vm = a.v[1][at], vz = a.v[2][at];
+    a.rl[0][at] = make_double2(vp.x - (dr2.x - tIm), vp.y - (dr2.y + tRe));
+    a.rl[1][at] = make_double2(vm.x - (dr2.x + tIm), vm.y - (dr2.y - tRe));
+    a.rl[2][at] = make_double2(vz.x - (-pv.y * kal), vz.y - (pv.x * kal));
+}
 
-// S4: warp = one (system, re/im) for 32 consecutive modes, so factor loads
-// are contiguous across the warp; LD factors are pivot-free
+// S4: warp = one (system, re/im) of 32 consecutive modes; LD never pivots
 __global__ void __launch_bounds__(192) k_solve_ld(StepArgs a) {
+    extern __shared__ double ring4[];
     const Geo &g = a.g;
     const int w = threadIdx.x >> 5;
     const int nh = blockIdx.x * 32 + (threadIdx.x & 31);
     const int sys = w >> 1, part = w & 1;
     if (nh >= g.H) return;
-    int k, m;
-    mode_km(nh, g.K, k, m);
-    RhsProj rhs{a.v[sys], a.p, a.dm.dr, a.dm.rp + 2 * g.N, g.N, g.Hp, nh, sys, part,
-                (double)(m * g.Mp), g.alpha * k};
+    const size_t st = 2 * (size_t)g.Hp;
+    const double *rhs = reinterpret_cast<const double *>(a.rl[sys]) + 2 * (size_t)nh + part;
     double *out = reinterpret_cast<double *>(a.v[sys]) + 2 * (size_t)nh + part;
     const double *lu = sys == 0 ? a.ldp : sys == 1 ? a.ldm : a.ldz;
-    solve_chain<false>(lu, nullptr, g.N, g.Hp, nh, rhs, out, 2 * (size_t)g.Hp);
+    solve_async<false>(lu, nullptr, g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x, blockDim.x);
 }
 
 // ------------------------------------------------------------------- S5
@@ -452,9 +486,13 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
         a.v[i] = ctx->s[i].d;
         a.u[i] = ctx->vel[i].d;
     }
-    a.p = ctx->s[3].d;
+    a.prhs = ctx->s[3].d;
+    a.p = ctx->s[4].d;
+    a.rl[0] = ctx->s[5].d;
+    a.rl[1] = ctx->s[6].d;
+    a.rl[2] = ctx->s[3].d;  // free once the pressure is solved
     a.lnp = ctx->LNp.lu;
-    a.pivp = ctx->LNp.piv;
+    a.pivd = ctx->LNp_pivd;
     a.ldp = ctx->LDp.lu;
     a.ldm = ctx->LDm.lu;
     a.ldz = ctx->LDz.lu;
@@ -470,6 +508,14 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
     a.const_flux = ctx->cfg.const_flux;
     a.sc = ctx->dsc;
     const unsigned tiles = grid1(g.H, TM);
+    static bool attrs_set = false;
+    if (!attrs_set) {
+        PF_CUDA(cudaFuncSetAttribute(k_solve_ld, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(192 * RING * (KL + 1) * sizeof(double))));
+        PF_CUDA(cudaFuncSetAttribute(k_solve_pnp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(64 * RING * (KV + 1) * sizeof(double))));
+        attrs_set = true;
+    }
     {
         ProfScope ps_(ctx, PF_K_STEP);
         k_step_rhs<<<tiles, TM * TR, (size_t)g.N * TM * sizeof(double2), ctx->stream>>>(a);
@@ -477,12 +523,17 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
     PF_LAUNCHED(ctx);
     {
         ProfScope ps_(ctx, PF_K_LUSOLVE);
-        k_solve_pnp<<<grid1(2LL * g.H, 128), 128, 0, ctx->stream>>>(a);
+        k_solve_pnp<<<tiles, 64, (size_t)64 * RING * (KV + 1) * sizeof(double), ctx->stream>>>(a);
+    }
+    PF_LAUNCHED(ctx);
+    {
+        ProfScope ps_(ctx, PF_K_STEP);
+        k_step_proj<<<dim3(grid1(g.H, 128), g.N), 128, 0, ctx->stream>>>(a);
     }
     PF_LAUNCHED(ctx);
     {
         ProfScope ps_(ctx, PF_K_LUSOLVE);
-        k_solve_ld<<<grid1(g.H, 32), 192, 0, ctx->stream>>>(a);
+        k_solve_ld<<<tiles, 192, (size_t)192 * RING * (KL + 1) * sizeof(double), ctx->stream>>>(a);
     }
     PF_LAUNCHED(ctx);
     if (corrector) PF_CUDA(cudaMemsetAsync(&ctx->dsc->dterr2_bits, 0, sizeof(unsigned long long), ctx->stream));
