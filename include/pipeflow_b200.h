@@ -138,6 +138,22 @@ int pf_tra_coll2phys(const pf_coll *c, pf_phys *p);
 /* tra_phys2spec + var_spec2coll (transform.fftw3.f90:108-147, variables.f90:281-294) */
 int pf_tra_phys2coll(const pf_phys *p, pf_coll *c);
 
+/* No counterpart in the reference.  The coll -> phys transform for callers
+ * that cannot allocate device memory (their device memory belongs to another
+ * allocator or pool, or they must not allocate inside their own step loop):
+ * no pf_ctx, no cudaMalloc/cudaFree.  re/im are the caller's DEVICE arrays in
+ * the coll host layout (re[nh*N + n]); phys is the caller's DEVICE output in
+ * the phys layout ([(n*3M + t)*3K + z]); the work is queued on cuda_stream
+ * (NULL = the legacy default stream).  Scratch is one static device array of
+ * PF_NOALLOC_SCRATCH_BYTES per GPU: sizes with N*M*3K*16 + 64 KiB above it,
+ * or with 3K or 3M outside {12,15,18,24,36,48,72,96,144,192,288,384}, are
+ * rejected with PF_ERR_ARG.  All calls share the scratch, so calls that
+ * overlap on the GPU race.  The first call on a device looks up the scratch
+ * address (cudaGetSymbolAddress); make it before any stream capture. */
+#define PF_NOALLOC_SCRATCH_BYTES (24u * 1024u * 1024u)
+int pf_tra_coll2phys_noalloc(int N, int K, int M, const double *re, const double *im,
+                             double *phys, void *cuda_stream);
+
 /* ---------------------------------------------------------- timestep.f90 */
 int pf_tim_get(const pf_ctx *ctx, pf_tim_state *s);
 int pf_tim_set(pf_ctx *ctx, const pf_tim_state *s);

@@ -87,6 +87,7 @@ _SIGS = {
     "pf_var_coll_norm": [P, DP, DP, DP],
     "pf_tra_coll2phys": [P, P],
     "pf_tra_phys2coll": [P, P],
+    "pf_tra_coll2phys_noalloc": [I, I, I, P, P, P, P],
     "pf_tim_get": [P, C.POINTER(pf_tim_state)],
     "pf_tim_set": [P, C.POINTER(pf_tim_state)],
     "pf_tim_mesh_init": [P, I, D, D, PP],
