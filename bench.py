@@ -192,6 +192,11 @@ def main():
             pipe.timestep()
         prof = pipe.prof_read()
         dom = max(prof, key=lambda k: prof[k][0])
+        # time only the dominant category from here on; the step graphs are
+        # re-captured (both pointer parities) with its event nodes, untimed
+        pipe.prof_enable([dom])
+        for _ in range(2):
+            pipe.timestep()
         pipe.prof_enable([dom])
         stream.synchronize()
         if dist:

@@ -53,7 +53,40 @@ int pf_phys_init_storage(pf_ctx *ctx, pf_phys *p) {
 
 void pf_events_release(pf_ctx *ctx);
 
+void pf_graphs_reset(pf_ctx *ctx) {
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int p = 0; p < 2; ++p) {
+        if (ctx->g_main[p]) cudaGraphExecDestroy(ctx->g_main[p]);
+        if (ctx->g_corr[p]) cudaGraphExecDestroy(ctx->g_corr[p]);
+        ctx->g_main[p] = ctx->g_corr[p] = nullptr;
+    }
+    for (int i = 0; i < 4; ++i) {
+        for (auto &e : ctx->g_ev[i]) {
+            ctx->ev_pool.push_back(e.second.first);
+            ctx->ev_pool.push_back(e.second.second);
+        }
+        ctx->g_ev[i].clear();
+    }
+    ctx->g_pending.clear();
+}
+
+// Accumulate the event pairs of the graphs replayed since the last sync.
+void pf_graph_events_collect(pf_ctx *ctx) {
+    for (int gi : ctx->g_pending)
+        for (auto &e : ctx->g_ev[gi]) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, e.second.first, e.second.second) == cudaSuccess) {
+                ctx->prof_ms[e.first] += ms;
+                ctx->prof_n[e.first] += 1;
+            } else {
+                cudaGetLastError();  // an unreadable pair must not surface at a later launch check
+            }
+        }
+    ctx->g_pending.clear();
+}
+
 static void free_all(pf_ctx *ctx) {
+    pf_graphs_reset(ctx);
     if (ctx->stream) pf_events_release(ctx);
     for (void *p : ctx->allocs) cudaFree(p);
     ctx->allocs.clear();
@@ -175,6 +208,7 @@ static int ctx_init(pf_ctx *ctx, const pf_config *cfg, int device) {
     ctx->lasterr = 1e99;
     ctx->newdt_i = 0;
     ctx->vel_nu = 1.0;
+    ctx->use_graphs = true;
     PF_CUDA(cudaStreamSynchronize(ctx->stream));
     return PF_OK;
 }
@@ -211,6 +245,7 @@ extern "C" int pf_ctx_destroy(pf_ctx *ctx) {
 extern "C" int pf_ctx_set_stream(pf_ctx *ctx, void *stream) {
     PF_ARG(ctx, "null ctx");
     PF_CUDA(cudaStreamSynchronize(ctx->stream));
+    pf_graphs_reset(ctx);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     if (stream) {
         ctx->stream = (cudaStream_t)stream;
@@ -502,8 +537,12 @@ static void prof_drain(pf_ctx *ctx) {
     for (int c = 0; c < PF_K_NCAT; ++c) {
         for (auto &pr : ctx->ev_open[c]) {
             float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) ctx->prof_ms[c] += ms;
-            ctx->prof_n[c] += 1;
+            if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) {
+                ctx->prof_ms[c] += ms;
+                ctx->prof_n[c] += 1;
+            } else {
+                cudaGetLastError();
+            }
             ctx->ev_pool.push_back(pr.first);
             ctx->ev_pool.push_back(pr.second);
         }
@@ -526,6 +565,8 @@ extern "C" int pf_ctx_launches(const pf_ctx *ctx, unsigned long long *n) {
 extern "C" int pf_prof_enable(pf_ctx *ctx, int mask) {
     PF_ARG(ctx, "null ctx");
     prof_drain(ctx);
+    pf_graph_events_collect(ctx);
+    if (mask != ctx->prof_mask) pf_graphs_reset(ctx);  // graphs bake in their event nodes
     for (int c = 0; c < PF_K_NCAT; ++c) {
         ctx->prof_ms[c] = 0.0;
         ctx->prof_n[c] = 0;
@@ -537,6 +578,7 @@ extern "C" int pf_prof_enable(pf_ctx *ctx, int mask) {
 extern "C" int pf_prof_read(pf_ctx *ctx, int cat, double *ms, unsigned long long *launches) {
     PF_ARG(ctx && cat >= 0 && cat < PF_K_NCAT, "pf_prof_read: bad argument");
     prof_drain(ctx);
+    pf_graph_events_collect(ctx);
     if (ms) *ms = ctx->prof_ms[cat];
     if (launches) *launches = ctx->prof_n[cat];
     return PF_OK;

@@ -168,6 +168,17 @@ struct pf_ctx {
     size_t T_bytes;
     int zinv_mc, zfwd_mc, th_zc;   // tile sizes
     std::vector<void *> allocs;    // everything to free
+    // CUDA graphs of the timestep: main[p] = imposesym, nonlinear terms,
+    // predictor, nonlinear terms, corrector starting from pointer parity p;
+    // corr[q] = nonlinear terms + corrector at parity q
+    int parity;                    // vel/prev pointer swap state
+    bool use_graphs, graph_warm;
+    cudaGraphExec_t g_main[2], g_corr[2];
+    unsigned long long g_main_n[2], g_corr_n[2];
+    // event pairs recorded inside each graph (profiled categories), and the
+    // graphs replayed since the last host synchronisation
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> g_ev[4];
+    std::vector<int> g_pending;
     // instrumentation
     unsigned long long launches;
     int prof_mask;
@@ -178,8 +189,18 @@ struct pf_ctx {
 };
 
 // Records a start/stop event pair around the launches in its scope when
-// profiling is enabled on the context.
+// profiling is enabled on the context.  While the stream is being captured
+// the records are made external, so the graph gets real event-record nodes
+// whose times can be read after each replay.
 cudaEvent_t pf_event_get(pf_ctx *ctx);
+inline void pf_event_record(cudaEvent_t e, cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &st);
+    if (st == cudaStreamCaptureStatusActive)
+        cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+    else
+        cudaEventRecord(e, s);
+}
 struct ProfScope {
     pf_ctx *ctx;
     int cat;
@@ -187,13 +208,13 @@ struct ProfScope {
     ProfScope(pf_ctx *c, int k) : ctx(c), cat(k), a(nullptr) {
         if (ctx->prof_mask & (1 << k)) {
             a = pf_event_get(ctx);
-            cudaEventRecord(a, ctx->stream);
+            pf_event_record(a, ctx->stream);
         }
     }
     ~ProfScope() {
         if (a) {
             cudaEvent_t b = pf_event_get(ctx);
-            cudaEventRecord(b, ctx->stream);
+            pf_event_record(b, ctx->stream);
             ctx->ev_open[cat].push_back({a, b});
         }
     }
@@ -253,3 +274,5 @@ int pf_norm_host(pf_ctx *ctx, const double2 *a, double *E, double *Ek, double *E
 bool pf_nl_fused_supported(const pf_ctx *ctx);
 int pf_launch_nl_fused(pf_ctx *ctx);
 int pf_vel_step_fused(pf_ctx *ctx, int corrector);
+void pf_graphs_reset(pf_ctx *ctx);
+void pf_graph_events_collect(pf_ctx *ctx);  // after a host sync

@@ -372,6 +372,7 @@ __global__ void k_piv_to_double(const unsigned char *__restrict__ piv, double *_
 // velocity.f90:120-146 including vel_adjustFlux(0) and vel_adjPPE(0)
 int pf_vel_matrices_impl(pf_ctx *ctx) {
     const Geo &g = ctx->g;
+    pf_graphs_reset(ctx);  // the graphs bake in 1/dt and the factor sets
     const pf_config &cfg = ctx->cfg;
     if (!ctx->LNp_set) {
         PF_TRY(lumesh_init(ctx, &ctx->LNp, 0, 1, 0.0, 1.0));

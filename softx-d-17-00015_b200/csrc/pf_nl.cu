@@ -71,13 +71,15 @@ __device__ __forceinline__ double2 nl_input(const NLArgs &a, int comp, int n, in
 template <int ZL, typename C>
 __global__ void __launch_bounds__(NL_THREADS) k_nl_zinv(NLArgs a, C *__restrict__ T, const C *__restrict__ twz, int MC) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    C *buf = reinterpret_cast<C *>(smraw);
-    C *tmp = buf + MC * ZL, *tw = tmp + MC * ZL;
+    using FR = FFTRows<ZL, C>;
+    constexpr int RS = FR::pitch;
+    C *rows = reinterpret_cast<C *>(smraw);
+    C *tw = rows + (FR::smem_elems(MC) - 2 * ZL), *tw2 = tw + ZL;
     const Geo &g = a.g;
     const int K = g.K;
     const int comp = blockIdx.z, n = blockIdx.y, m0 = blockIdx.x * MC;
     const int mc = min(MC, g.M - m0);
-    for (int i = threadIdx.x; i < ZL; i += blockDim.x) tw[i] = twz[i];
+    fft4_tables<ZL>(tw, tw2, twz);
     for (int idx = threadIdx.x; idx < mc * ZL; idx += blockDim.x) {
         const int c = idx / ZL, j = idx - c * ZL;
         const int m = m0 + c;
@@ -92,12 +94,15 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_zinv(NLArgs a, C *__restrict_
             const int kk = j < K ? j : (j >= 2 * K + 1 ? j - ZL : K);
             if (kk < K) v = nl_input(a, comp, n, m * (2 * K - 1) + kk, kk, m);
         }
-        buf[idx] = to_c<C>(v);
+        rows[c * RS + j] = to_c<C>(v);
     }
     __syncthreads();
-    const C *res = smem_fft_t<ZL, +1>(buf, tmp, mc, tw);
+    FR::template run<+1>(rows, mc, tw, tw2);
     C *out = T + ((size_t)(comp * g.N + n) * g.M + m0) * ZL;
-    for (int idx = threadIdx.x; idx < mc * ZL; idx += blockDim.x) out[idx] = res[idx];
+    for (int idx = threadIdx.x; idx < mc * ZL; idx += blockDim.x) {
+        const int c = idx / ZL, j = idx - c * ZL;
+        out[idx] = rows[c * RS + j];
+    }
 }
 
 __device__ __forceinline__ void atomic_max_pos(unsigned long long *p, double v) {
@@ -109,14 +114,17 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_theta(NLArgs a, C *__restrict
                                                          int ZC, typename CTraits<C>::R scale) {
     using R = typename CTraits<C>::R;
     extern __shared__ __align__(16) unsigned char smraw[];
+    using FR = FFTRows<TL, C>;
+    constexpr int RS = FR::pitch;
     const Geo &g = a.g;
     const int M = g.M, Z = g.Z, np = ZC / 2;
     const int rowsA = 3 * ZC;  // six components x ZC/2 packed pairs
     C *bufA = reinterpret_cast<C *>(smraw);
-    C *bufB = bufA + rowsA * TL, *tw = bufB + rowsA * TL;
+    C *bufB = bufA + (FR::smem_elems(rowsA) - 2 * TL);
+    C *tw = bufB + (FR::smem_elems(rowsA / 2) - 2 * TL), *tw2 = tw + TL;
     const int n = blockIdx.y, z0 = blockIdx.x * ZC;
-    for (int i = threadIdx.x; i < TL; i += blockDim.x) tw[i] = twt[i];
-    for (int i = threadIdx.x; i < rowsA * TL; i += blockDim.x) bufA[i] = CTraits<C>::make(0, 0);
+    fft4_tables<TL>(tw, tw2, twt);
+    for (int i = threadIdx.x; i < rowsA * RS; i += blockDim.x) bufA[i] = CTraits<C>::make(0, 0);
     __syncthreads();
     // Hermitian-extend the M retained theta modes of two z rows into one
     // complex row: X = a + i b (c2r ignores the DC imaginary parts)
@@ -127,7 +135,7 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_theta(NLArgs a, C *__restrict
         const C *col = T + ((size_t)(comp * g.N + n) * M + m) * Z;
         const C va = (za < Z) ? col[za] : CTraits<C>::make(0, 0);
         const C vb = (zb < Z) ? col[zb] : CTraits<C>::make(0, 0);
-        C *X = bufA + (comp * np + zp) * TL;
+        C *X = bufA + (comp * np + zp) * RS;
         if (m == 0) {
             X[0] = CTraits<C>::make(va.x, vb.x);
         } else {
@@ -136,8 +144,9 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_theta(NLArgs a, C *__restrict
         }
     }
     __syncthreads();
-    C *phys = smem_fft_t<TL, +1>(bufA, bufB, rowsA, tw);
-    C *prod = (phys == bufA) ? bufB : bufA;
+    FR::template run<+1>(bufA, rowsA, tw, tw2);
+    const C *phys = bufA;
+    C *prod = bufB;
     // u x curl(u) (velocity.f90:325-329), scaled for the forward transform
     const R base = (R)(1.0 - a.dm.rp[4 * g.N + n] * a.dm.rp[4 * g.N + n]);
     R mr = 0, mt = 0, mz = 0;
@@ -145,7 +154,7 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_theta(NLArgs a, C *__restrict
         const int zp = idx / TL, t = idx - zp * TL;
         C u[6];
 #pragma unroll
-        for (int c = 0; c < 6; ++c) u[c] = phys[(c * np + zp) * TL + t];
+        for (int c = 0; c < 6; ++c) u[c] = phys[(c * np + zp) * RS + t];
         // .x holds row za, .y row zb
         const C pr = CTraits<C>::make((u[1].x * u[5].x - u[2].x * u[4].x) * scale,
                                       (u[1].y * u[5].y - u[2].y * u[4].y) * scale);
@@ -153,9 +162,9 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_theta(NLArgs a, C *__restrict
                                       (u[2].y * u[3].y - u[0].y * u[5].y) * scale);
         const C pz = CTraits<C>::make((u[0].x * u[4].x - u[1].x * u[3].x) * scale,
                                       (u[0].y * u[4].y - u[1].y * u[3].y) * scale);
-        prod[(0 * np + zp) * TL + t] = pr;
-        prod[(1 * np + zp) * TL + t] = pt;
-        prod[(2 * np + zp) * TL + t] = pz;
+        prod[(0 * np + zp) * RS + t] = pr;
+        prod[(1 * np + zp) * RS + t] = pt;
+        prod[(2 * np + zp) * RS + t] = pz;
         const bool hasb = z0 + 2 * zp + 1 < Z;
         mr = fmax(mr, fmax(fabs(u[0].x), hasb ? fabs(u[0].y) : (R)0));
         mt = fmax(mt, fmax(fabs(u[1].x), hasb ? fabs(u[1].y) : (R)0));
@@ -174,12 +183,12 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_theta(NLArgs a, C *__restrict
         }
     }
     __syncthreads();
-    C *res = smem_fft_t<TL, -1>(prod, phys, 3 * np, tw);
+    FR::template run<-1>(prod, 3 * np, tw, tw2);
     // separate the two packed real transforms and keep m < M
     for (int idx = threadIdx.x; idx < 3 * M * np; idx += blockDim.x) {
         const int zp = idx % np, rest = idx / np;
         const int m = rest % M, comp = rest / M;
-        const C *X = res + (comp * np + zp) * TL;
+        const C *X = prod + (comp * np + zp) * RS;
         const C A = X[m], B = X[(TL - m) % TL];
         const C va = CTraits<C>::make((R)0.5 * (A.x + B.x), (R)0.5 * (A.y - B.y));
         const C vb = CTraits<C>::make((R)0.5 * (A.y + B.y), (R)-0.5 * (A.x - B.x));
@@ -194,17 +203,23 @@ template <int ZL, typename C>
 __global__ void __launch_bounds__(NL_THREADS) k_nl_zfwd(NLArgs a, const C *__restrict__ T, const C *__restrict__ twz,
                                                         int MC) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    C *buf = reinterpret_cast<C *>(smraw);
-    C *tmp = buf + MC * ZL, *tw = tmp + MC * ZL;
+    using FR = FFTRows<ZL, C>;
+    constexpr int RS = FR::pitch;
+    C *rows = reinterpret_cast<C *>(smraw);
+    C *tw = rows + (FR::smem_elems(MC) - 2 * ZL), *tw2 = tw + ZL;
     const Geo &g = a.g;
     const int K = g.K;
     const int comp = blockIdx.z, n = blockIdx.y, m0 = blockIdx.x * MC;
     const int mc = min(MC, g.M - m0);
-    for (int i = threadIdx.x; i < ZL; i += blockDim.x) tw[i] = twz[i];
+    fft4_tables<ZL>(tw, tw2, twz);
     const C *in = T + ((size_t)(comp * g.N + n) * g.M + m0) * ZL;
-    for (int idx = threadIdx.x; idx < mc * ZL; idx += blockDim.x) buf[idx] = in[idx];
+    for (int idx = threadIdx.x; idx < mc * ZL; idx += blockDim.x) {
+        const int c = idx / ZL, j = idx - c * ZL;
+        rows[c * RS + j] = in[idx];
+    }
     __syncthreads();
-    const C *res = smem_fft_t<ZL, -1>(buf, tmp, mc, tw);
+    FR::template run<-1>(rows, mc, tw, tw2);
+    const C *res = rows;
     const double U = a.dm.velU[n], b = -a.dm.velUp[n];
     double Pr0 = 0.0;
     if (comp == 2 && a.const_flux) {
@@ -218,7 +233,7 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_zfwd(NLArgs a, const C *__res
         const int m = m0 + c;
         if (m == 0 && kk < 0) continue;
         const int nh = m * (2 * K - 1) + kk;
-        const C x = res[c * ZL + (kk >= 0 ? kk : ZL + kk)];
+        const C x = res[c * RS + (kk >= 0 ? kk : ZL + kk)];
         const size_t at = (size_t)n * g.Hp + nh;
         const double av = g.alpha * kk * U;
         double2 o = make_double2((double)x.x, (double)x.y);
@@ -252,23 +267,40 @@ static bool nl_length_ok(int L) {
 
 bool pf_nl_fused_supported(const pf_ctx *ctx) { return nl_length_ok(ctx->g.Z) && nl_length_ok(ctx->g.Th); }
 
+// shared-memory elements of B transform rows (plus tables) for a built length
+template <typename C> static int rows_elems(int L, int B) {
+    switch (L) {
+#define PF_CASE(L) \
+    case L:        \
+        return FFTRows<L, C>::smem_elems(B);
+        PF_NL_LENGTHS(PF_CASE)
+#undef PF_CASE
+    default:
+        return 2 * B * L + 2 * L;
+    }
+}
+
 template <typename C>
 static int launch_nl(pf_ctx *ctx, const NLArgs &a, const C *twz, const C *twt) {
     const Geo &g = ctx->g;
     C *T = reinterpret_cast<C *>(ctx->T);
     const size_t cs = sizeof(C);
     int MC = g.M;
-    while (MC > 1 && (size_t)(2 * MC + 1) * g.Z * cs > 60 * 1024) --MC;
-    const size_t zsm = (size_t)(2 * MC + 1) * g.Z * cs;
+    while (MC > 1 && (size_t)rows_elems<C>(g.Z, MC) * cs > 64 * 1024) --MC;
+    const size_t zsm = (size_t)rows_elems<C>(g.Z, MC) * cs;
     int ZC = 8;
-    while (ZC > 2 && ((size_t)2 * 3 * ZC + 1) * g.Th * cs > 60 * 1024) ZC -= 2;
-    const size_t tsm = ((size_t)2 * 3 * ZC + 1) * g.Th * cs;
+    while (ZC > 2 && (size_t)(rows_elems<C>(g.Th, 3 * ZC) + rows_elems<C>(g.Th, 3 * ZC / 2)) * cs > 64 * 1024) ZC -= 2;
+    const size_t tsm = (size_t)(rows_elems<C>(g.Th, 3 * ZC) + rows_elems<C>(g.Th, 3 * ZC / 2)) * cs;
     const dim3 gz((g.M + MC - 1) / MC, g.N, 6), gt((g.Z + ZC - 1) / ZC, g.N), gf((g.M + MC - 1) / MC, g.N, 3);
     const typename CTraits<C>::R scale = (typename CTraits<C>::R)(1.0 / (double)(g.Z * g.Th));
     switch (g.Z) {
 #define PF_CASE(L)                                                                                   \
     case L: {                                                                                        \
-        PF_CUDA(cudaFuncSetAttribute(k_nl_zinv<L, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsm)); \
+        static size_t set_ = 0;                                                                      \
+        if (zsm > set_) {                                                                              \
+            PF_CUDA(cudaFuncSetAttribute(k_nl_zinv<L, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsm)); \
+            set_ = zsm;                                                                               \
+        }                                                                                            \
         ProfScope ps_(ctx, PF_K_ZINV);                                                               \
         k_nl_zinv<L, C><<<gz, NL_THREADS, zsm, ctx->stream>>>(a, T, twz, MC);                        \
     } break;
@@ -283,7 +315,11 @@ static int launch_nl(pf_ctx *ctx, const NLArgs &a, const C *twz, const C *twt) {
     switch (g.Th) {
 #define PF_CASE(L)                                                                                    \
     case L: {                                                                                         \
-        PF_CUDA(cudaFuncSetAttribute(k_nl_theta<L, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm)); \
+        static size_t set_ = 0;                                                                      \
+        if (tsm > set_) {                                                                              \
+            PF_CUDA(cudaFuncSetAttribute(k_nl_theta<L, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm)); \
+            set_ = tsm;                                                                               \
+        }                                                                                            \
         ProfScope ps_(ctx, PF_K_THFWD);                                                               \
         k_nl_theta<L, C><<<gt, NL_THREADS, tsm, ctx->stream>>>(a, T, twt, ZC, scale);                 \
     } break;
@@ -297,7 +333,11 @@ static int launch_nl(pf_ctx *ctx, const NLArgs &a, const C *twz, const C *twt) {
     switch (g.Z) {
 #define PF_CASE(L)                                                                                   \
     case L: {                                                                                        \
-        PF_CUDA(cudaFuncSetAttribute(k_nl_zfwd<L, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsm)); \
+        static size_t set_ = 0;                                                                      \
+        if (zsm > set_) {                                                                              \
+            PF_CUDA(cudaFuncSetAttribute(k_nl_zfwd<L, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsm)); \
+            set_ = zsm;                                                                               \
+        }                                                                                            \
         ProfScope ps_(ctx, PF_K_ZFWD);                                                               \
         k_nl_zfwd<L, C><<<gf, NL_THREADS, zsm, ctx->stream>>>(a, T, twz, MC);                        \
     } break;

@@ -476,8 +476,10 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
         pf_set_error("fused step: Helmholtz factors pivoted");
         return PF_ERR_STATE;
     }
-    if (!corrector)
+    if (!corrector) {
         for (int i = 0; i < 3; ++i) std::swap(ctx->vel[i].d, ctx->prev[i].d);
+        ctx->parity ^= 1;
+    }
     StepArgs a;
     for (int i = 0; i < 3; ++i) {
         a.u_[i] = ctx->prev[i].d;

@@ -117,6 +117,7 @@ static int vel_corrector_async(pf_ctx *ctx) {
 static int read_dterr(pf_ctx *ctx) {
     PF_CUDA(cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream));
     PF_CUDA(cudaStreamSynchronize(ctx->stream));
+    pf_graph_events_collect(ctx);
     const double d2 = bits_to_double(ctx->hsc->dterr2_bits);
     ctx->tim.dterr = std::max(ctx->tim.dterr, std::sqrt(d2));
     return PF_OK;
@@ -208,25 +209,115 @@ extern "C" int pf_tim_new_tstep(pf_ctx *ctx) {
 }
 
 // main.f90:20-44
+// Capture `body` on the context stream into an executable graph; the
+// context's profiling is paused so no event pairs are recorded, and the
+// number of kernels captured is returned in *nk.
+// Capture `body` on the context stream into an executable graph.  Event
+// pairs of profiled categories become event-record nodes of the graph (kept
+// in ctx->g_ev[slot]); *nk returns the number of kernels captured.
+template <typename F>
+static int capture(pf_ctx *ctx, int slot, cudaGraphExec_t *exec, unsigned long long *nk, F body) {
+    const unsigned long long n0 = ctx->launches;
+    size_t open0[PF_K_NCAT];
+    for (int c = 0; c < PF_K_NCAT; ++c) open0[c] = ctx->ev_open[c].size();
+    cudaGraph_t graph = nullptr;
+    PF_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const int s = body();
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    for (int c = 0; c < PF_K_NCAT; ++c) {  // move the captured pairs to the graph's list
+        for (size_t i = open0[c]; i < ctx->ev_open[c].size(); ++i) ctx->g_ev[slot].push_back({c, ctx->ev_open[c][i]});
+        ctx->ev_open[c].resize(open0[c]);
+    }
+    if (s != PF_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return s;
+    }
+    if (e != cudaSuccess) {
+        pf_set_error("graph capture failed: %s", cudaGetErrorString(e));
+        return PF_ERR_CUDA;
+    }
+    const cudaError_t e2 = cudaGraphInstantiate(exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) {
+        pf_set_error("graph instantiation failed: %s", cudaGetErrorString(e2));
+        return PF_ERR_CUDA;
+    }
+    *nk = ctx->launches - n0;
+    ctx->launches = n0;  // counted again at each replay
+    return PF_OK;
+}
+
+static int replay(pf_ctx *ctx, int slot, cudaGraphExec_t g, unsigned long long nk) {
+    PF_CUDA(cudaGraphLaunch(g, ctx->stream));
+    ctx->launches += nk;
+    if (!ctx->g_ev[slot].empty()) ctx->g_pending.push_back(slot);
+    return PF_OK;
+}
+
+static bool graphs_ok(const pf_ctx *ctx) {
+    return ctx->use_graphs && ctx->cfg.dt > 0.0 && pf_nl_fused_supported(ctx) && fused_step_ok(ctx);
+}
+
+// main.f90:20-44.  With a fixed dt and the fused kernels, the pass through
+// predictor and first corrector is one graph launch and each further
+// corrector pass another; the corrector error is read once per pass.
 extern "C" int pf_timestep(pf_ctx *ctx, int *ncorr) {
     PF_ARG(ctx, "null ctx");
     PF_TRY(require_matrices(ctx));
-    PF_TRY(pf_vel_imposesym(ctx));
-    PF_TRY(transform_nonlinear(ctx));
-    if (ctx->cfg.dt < 0.0) {
-        PF_TRY(pf_vel_maxtstep(ctx));
-        PF_TRY(pf_tim_new_tstep(ctx));
-        if (ctx->tim.new_dt) PF_TRY(pf_vel_matrices_impl(ctx));
-    }
-    PF_TRY(pf_vel_predictor(ctx));
-    ctx->tim.it = 1;
     int nc = 0, status = PF_OK;
-    while (ctx->tim.it != 0) {
+    // the first step of a context runs eagerly: it sets every kernel's
+    // shared-memory attribute, which must not happen during a capture
+    if (graphs_ok(ctx) && ctx->graph_warm) {
+        const int p = ctx->parity;
+        if (!ctx->g_main[p]) {
+            PF_TRY(capture(ctx, p, &ctx->g_main[p], &ctx->g_main_n[p], [&]() {
+                PF_TRY(pf_vel_imposesym(ctx));
+                PF_TRY(transform_nonlinear(ctx));
+                PF_TRY(pf_vel_step_fused(ctx, 0));
+                PF_TRY(transform_nonlinear(ctx));
+                return pf_vel_step_fused(ctx, 1);
+            }));
+            // capture swapped the host pointers; the replay below does it for real
+            for (int i = 0; i < 3; ++i) std::swap(ctx->vel[i].d, ctx->prev[i].d);
+            ctx->parity = p;
+        }
+        PF_TRY(replay(ctx, p, ctx->g_main[p], ctx->g_main_n[p]));
+        for (int i = 0; i < 3; ++i) std::swap(ctx->vel[i].d, ctx->prev[i].d);
+        ctx->parity = p ^ 1;
+        ctx->cfl_fused = true;
+        ctx->tim.it = 1;
+        for (;;) {
+            PF_TRY(read_dterr(ctx));
+            const int s = pf_tim_check_cgce(ctx);
+            if (s != PF_OK) status = s;
+            ++nc;
+            if (ctx->tim.it == 0) break;
+            const int q = ctx->parity;
+            if (!ctx->g_corr[q])
+                PF_TRY(capture(ctx, 2 + q, &ctx->g_corr[q], &ctx->g_corr_n[q], [&]() {
+                    PF_TRY(transform_nonlinear(ctx));
+                    return pf_vel_step_fused(ctx, 1);
+                }));
+            PF_TRY(replay(ctx, 2 + q, ctx->g_corr[q], ctx->g_corr_n[q]));
+        }
+    } else {
+        PF_TRY(pf_vel_imposesym(ctx));
         PF_TRY(transform_nonlinear(ctx));
-        PF_TRY(pf_vel_corrector(ctx));
-        const int s = pf_tim_check_cgce(ctx);
-        if (s != PF_OK) status = s;
-        ++nc;
+        if (ctx->cfg.dt < 0.0) {
+            PF_TRY(pf_vel_maxtstep(ctx));
+            PF_TRY(pf_tim_new_tstep(ctx));
+            if (ctx->tim.new_dt) PF_TRY(pf_vel_matrices_impl(ctx));
+        }
+        PF_TRY(pf_vel_predictor(ctx));
+        ctx->tim.it = 1;
+        while (ctx->tim.it != 0) {
+            PF_TRY(transform_nonlinear(ctx));
+            PF_TRY(pf_vel_corrector(ctx));
+            const int s = pf_tim_check_cgce(ctx);
+            if (s != PF_OK) status = s;
+            ++nc;
+        }
+        ctx->graph_warm = graphs_ok(ctx);
     }
     ctx->tim.t = ctx->tim.t + ctx->tim.dt;
     ctx->tim.step = ctx->tim.step + 1;

@@ -271,3 +271,24 @@ def test_steporbit_parity(cfgd):
         o.timestep(orbit=True)
     g.steporbit(4)
     assert O.rel_l2(state_from_dev(g), o.state()) <= 1e-12
+
+
+def test_multi_corrector_graph_path_parity():
+    """A tight corrector tolerance forces several corrector passes per step,
+    exercising the replayed corrector graphs at both pointer parities."""
+    cfgd = dict(SMALL[0], dterr=1e-9)
+    o, g = oracle_pipe(cfgd), device_pipe(cfgd)
+    o.vel_matrices()
+    g.vel_matrices()
+    st = O.seeded_state(o, 6, 1e-2)
+    o.set_state(*st)
+    state_to_dev(g, st)
+    counts = []
+    for _ in range(4):
+        nco = o.timestep()
+        ncg = g.timestep()
+        assert nco == ncg
+        counts.append(ncg)
+    assert max(counts) >= 2
+    assert O.rel_l2(state_from_dev(g), o.state()) <= 1e-12
+    assert g.launches() > 0
