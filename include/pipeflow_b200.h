@@ -199,6 +199,10 @@ int pf_vel_imposesym(pf_ctx *ctx);                                  /* :61-74 */
 int pf_vel_matrices(pf_ctx *ctx);                                   /* :120-146 */
 int pf_vel_transform(pf_ctx *ctx);                                  /* :304-317 */
 int pf_vel_nonlinear(pf_ctx *ctx);                                  /* :323-335 */
+/* vel_transform + vel_nonlinear fused (velocity.f90:304-361): N from u in
+ * three launches without materialising vel_r..vel_curlz (those module
+ * fields are not updated); CFL maxima are kept for pf_vel_maxtstep. */
+int pf_vel_transform_nonlinear(pf_ctx *ctx);
 int pf_vel_predictor(pf_ctx *ctx);                                  /* :400-410 */
 int pf_vel_corrector(pf_ctx *ctx);                                  /* :416-432 */
 int pf_vel_maxtstep(pf_ctx *ctx);                                   /* :438-481 */
@@ -218,6 +222,26 @@ int pf_steporbit(pf_ctx *ctx, int nsteps);
 /* Perturbation energy and friction diagnostics of io.f90:501-514, 627-639. */
 int pf_diag_energy(pf_ctx *ctx, double *E);
 int pf_diag_friction(pf_ctx *ctx, double *Ub, double *Uc, double *Ufr);
+
+/* ----------------------------------------------------------------- batches */
+/* Many independent pipes of uneven (N, K, M, Re, alpha, dt) advanced together;
+ * one timestep of the batch is a single CUDA graph with one kernel chain per
+ * pipe.  Each pipe's arithmetic is the lone-pipe path, so results are the
+ * same alone and in the batch.  No single reference routine: this drives
+ * the main.f90 loop body (main.f90:20-44) or steporbit's (newton.f90:740-762)
+ * for every pipe. */
+typedef struct pf_batch pf_batch;
+int pf_batch_create(int npipes, const pf_config *cfgs, int device, pf_batch **out);
+int pf_batch_destroy(pf_batch *b);
+/* The context of pipe i (owned by the batch): set its state, read results. */
+int pf_batch_pipe(pf_batch *b, int i, pf_ctx **out);
+/* vel_matrices for every pipe. */
+int pf_batch_matrices(pf_batch *b);
+/* nsteps timesteps of every pipe; orbit=0 iterates each pipe's corrector to
+ * convergence, orbit=1 takes exactly one corrector pass.  *corr_passes
+ * (may be NULL) = corrector passes summed over pipes and steps. */
+int pf_batch_step(pf_batch *b, int nsteps, int orbit, long long *corr_passes);
+int pf_batch_sync(pf_batch *b);
 
 /* ------------------------------------------------------- instrumentation */
 /* Kernel categories timed by CUDA events when profiling is on (the reference

@@ -275,4 +275,7 @@ bool pf_nl_fused_supported(const pf_ctx *ctx);
 int pf_launch_nl_fused(pf_ctx *ctx);
 int pf_vel_step_fused(pf_ctx *ctx, int corrector);
 void pf_graphs_reset(pf_ctx *ctx);
+int pf_transform_nonlinear(pf_ctx *ctx);
+int pf_read_dterr(pf_ctx *ctx);
+bool pf_fused_step_ok(const pf_ctx *ctx);
 void pf_graph_events_collect(pf_ctx *ctx);  // after a host sync

@@ -350,6 +350,8 @@ static int launch_nl(pf_ctx *ctx, const NLArgs &a, const C *twz, const C *twt) {
     return PF_OK;
 }
 
+__global__ void k_nl_mean64(NLArgs a);
+
 // vel_transform + vel_nonlinear in three launches; CFL maxima per radial
 // point are left in ctx->cflmax.
 int pf_launch_nl_fused(pf_ctx *ctx) {
@@ -363,7 +365,64 @@ int pf_launch_nl_fused(pf_ctx *ctx) {
     a.const_flux = ctx->cfg.const_flux;
     a.sc = ctx->dsc;
     a.cfl = ctx->cflmax;
-    if (ctx->cfg.precision == PF_PREC_MIXED)
-        return launch_nl<float2>(ctx, a, ctx->twZf, ctx->twTf);
+    if (ctx->cfg.precision == PF_PREC_MIXED) {
+        PF_TRY(launch_nl<float2>(ctx, a, ctx->twZf, ctx->twTf));
+        {
+            ProfScope ps_(ctx, PF_K_ZFWD);
+            k_nl_mean64<<<ctx->g.N, 256, 0, ctx->stream>>>(a);
+        }
+        PF_LAUNCHED(ctx);
+        return PF_OK;
+    }
     return launch_nl<double2>(ctx, a, ctx->twZ, ctx->twT);
+}
+
+// ------------------------------------------------- FP64 mean mode (mixed)
+// With FP32 transforms the k=m=0 coefficient of u x curl(u) is replaced by
+// its exact FP64 value.  On the 3/2-dealiased grid no product of retained
+// modes aliases onto (0,0), so the grid mean equals the spectral sum
+//   mean(f g) = Re f00 Re g00 + 2 sum_{k>=1} Re(f_k0 conj g_k0)
+//             + 2 sum_{m>=1, all k} Re(f_km conj g_km)
+// (the c2r transform ignores Im f00).  One block per radial point.
+__global__ void k_nl_mean64(NLArgs a) {
+    const Geo &g = a.g;
+    const int n = blockIdx.x;
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int nh = threadIdx.x; nh < g.H; nh += blockDim.x) {
+        int k, m;
+        mode_km(nh, g.K, k, m);
+        double2 u[6];
+        for (int c = 0; c < 6; ++c) u[c] = nl_input(a, c, n, nh, k, m);
+        const double w = (nh == 0) ? 1.0 : 2.0;
+        auto dot = [&](double2 f, double2 h) { return nh == 0 ? f.x * h.x : f.x * h.x + f.y * h.y; };
+        s[0] += w * (dot(u[1], u[5]) - dot(u[2], u[4]));
+        s[1] += w * (dot(u[2], u[3]) - dot(u[0], u[5]));
+        s[2] += w * (dot(u[0], u[4]) - dot(u[1], u[3]));
+    }
+    __shared__ double red[3][32];
+    for (int c = 0; c < 3; ++c) {
+        double v = s[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) red[c][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t[3] = {0.0, 0.0, 0.0};
+        for (int c = 0; c < 3; ++c)
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t[c] += red[c][i];
+        const size_t at = (size_t)n * g.Hp;  // nh = 0
+        // vel_addHPF at k=m=0: a = 0; N_z += -U' u_r (u_r(0,0) is zero after
+        // imposesym but kept for fidelity) and the constant-flux pressure
+        const double2 ur = a.u[0][at];
+        double zr = t[2] + (-a.dm.velUp[n]) * ur.x;
+        if (a.const_flux) {
+            double Pr0 = 0.0;
+            for (int j = 0; j <= KL; ++j) Pr0 += a.u[2][(size_t)(g.N - 1 - KL + j) * g.Hp].x * a.dm.dr1[1 * (KL + 1) + j];
+            Pr0 = Pr0 / (-2.0);
+            zr = zr + 4.0 * Pr0 / g.Re;
+        }
+        a.N[0][at] = make_double2(t[0], 0.0);
+        a.N[1][at] = make_double2(t[1], 0.0);
+        a.N[2][at] = make_double2(zr, (-a.dm.velUp[n]) * ur.y);
+    }
 }

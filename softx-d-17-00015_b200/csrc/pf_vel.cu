@@ -86,7 +86,9 @@ static int vel_step(pf_ctx *ctx) {
     return pf_launch_zero_mode0(ctx);
 }
 
-static bool fused_step_ok(const pf_ctx *ctx) {
+bool pf_fused_step_ok(const pf_ctx *ctx);
+static bool fused_step_ok(const pf_ctx *ctx) { return pf_fused_step_ok(ctx); }
+bool pf_fused_step_ok(const pf_ctx *ctx) {
     return ctx->g.N <= 128 && !ctx->LDp.pivoted && !ctx->LDm.pivoted && !ctx->LDz.pivoted;
 }
 
@@ -114,7 +116,9 @@ static int vel_corrector_async(pf_ctx *ctx) {
                                  ctx->save[2].d, ctx->vel[2].d, true);
 }
 
-static int read_dterr(pf_ctx *ctx) {
+int pf_read_dterr(pf_ctx *ctx);
+static int read_dterr(pf_ctx *ctx) { return pf_read_dterr(ctx); }
+int pf_read_dterr(pf_ctx *ctx) {
     PF_CUDA(cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream));
     PF_CUDA(cudaStreamSynchronize(ctx->stream));
     pf_graph_events_collect(ctx);
@@ -131,7 +135,9 @@ extern "C" int pf_vel_corrector(pf_ctx *ctx) {
 
 // vel_transform + vel_nonlinear for the drivers: the fused three-launch
 // path when the transform lengths are instantiated, else the materialising one
-static int transform_nonlinear(pf_ctx *ctx) {
+int pf_transform_nonlinear(pf_ctx *ctx);
+static int transform_nonlinear(pf_ctx *ctx) { return pf_transform_nonlinear(ctx); }
+int pf_transform_nonlinear(pf_ctx *ctx) {
     if (pf_nl_fused_supported(ctx)) {
         PF_TRY(pf_launch_nl_fused(ctx));
         ctx->cfl_fused = true;
@@ -139,6 +145,11 @@ static int transform_nonlinear(pf_ctx *ctx) {
     }
     PF_TRY(pf_vel_transform(ctx));
     return pf_vel_nonlinear(ctx);
+}
+
+extern "C" int pf_vel_transform_nonlinear(pf_ctx *ctx) {
+    PF_ARG(ctx, "null ctx");
+    return pf_transform_nonlinear(ctx);
 }
 
 extern "C" int pf_vel_maxtstep(pf_ctx *ctx) {

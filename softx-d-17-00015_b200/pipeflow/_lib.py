@@ -112,6 +112,7 @@ _SIGS = {
     "pf_vel_matrices": [P],
     "pf_vel_transform": [P],
     "pf_vel_nonlinear": [P],
+    "pf_vel_transform_nonlinear": [P],
     "pf_vel_predictor": [P],
     "pf_vel_corrector": [P],
     "pf_vel_maxtstep": [P],
@@ -120,6 +121,12 @@ _SIGS = {
     "pf_steporbit": [P, I],
     "pf_diag_energy": [P, DP],
     "pf_diag_friction": [P, DP, DP, DP],
+    "pf_batch_create": [I, C.POINTER(pf_config), I, PP],
+    "pf_batch_destroy": [P],
+    "pf_batch_pipe": [P, I, PP],
+    "pf_batch_matrices": [P],
+    "pf_batch_step": [P, I, I, C.POINTER(C.c_longlong)],
+    "pf_batch_sync": [P],
     "pf_ctx_launches": [P, C.POINTER(C.c_ulonglong)],
     "pf_prof_enable": [P, I],
     "pf_prof_read": [P, I, DP, C.POINTER(C.c_ulonglong)],

@@ -72,6 +72,23 @@ class PipeConfig:
         return 3 * self.M
 
 
+def cfg_struct(cfg: PipeConfig) -> L.pf_config:
+    """The C ABI configuration record of a PipeConfig (keeps a custom mesh alive)."""
+    c = L.pf_config()
+    for f in ("N", "K", "M", "Mp", "Re", "alpha", "dt", "implicit", "dterr", "courant", "maxdt"):
+        setattr(c, f, getattr(cfg, f))
+    c.const_flux = int(cfg.const_flux)
+    c.mirrorsym = int(cfg.mirrorsym)
+    c.shiftrefl = int(cfg.shiftrefl)
+    c.shiftrott = int(cfg.shiftrott)
+    c.precision = int(cfg.precision)
+    c._r = None
+    if cfg.r is not None:
+        c._r = np.ascontiguousarray(cfg.r, dtype=np.float64)
+        c.r = _dp(c._r)
+    return c
+
+
 class Coll:
     """A device `type (coll)` field (variables.f90:37-40)."""
 
@@ -180,34 +197,28 @@ class LUMesh:
 class Pipe:
     """Module state of one pipe on one GPU."""
 
-    def __init__(self, cfg: PipeConfig, device: int = -1):
+    def __init__(self, cfg: PipeConfig, device: int = -1, _handle=None):
         self.lib = L.load()
         self.cfg = cfg
-        c = L.pf_config()
-        for f in ("N", "K", "M", "Mp", "Re", "alpha", "dt", "implicit", "dterr", "courant", "maxdt"):
-            setattr(c, f, getattr(cfg, f))
-        c.const_flux = int(cfg.const_flux)
-        c.mirrorsym = int(cfg.mirrorsym)
-        c.shiftrefl = int(cfg.shiftrefl)
-        c.shiftrott = int(cfg.shiftrott)
-        c.precision = int(cfg.precision)
-        self._r = None
-        if cfg.r is not None:
-            self._r = np.ascontiguousarray(cfg.r, dtype=np.float64)
-            c.r = _dp(self._r)
+        self._owned = _handle is None
         self.ctx = None
-        h = C.c_void_p()
-        _check(self.lib.pf_ctx_create(C.byref(c), device, C.byref(h)))
-        self.ctx = h
+        if _handle is None:
+            c = cfg_struct(cfg)
+            self._r = c._r
+            h = C.c_void_p()
+            _check(self.lib.pf_ctx_create(C.byref(c), device, C.byref(h)))
+            self.ctx = h
+        else:
+            self.ctx = _handle
         N, H, Z, Th = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         _check(self.lib.pf_ctx_dims(self.ctx, C.byref(N), C.byref(H), C.byref(Z), C.byref(Th)))
         self.N, self.H, self.Z, self.Th = N.value, H.value, Z.value, Th.value
         self.K, self.M, self.Mp = cfg.K, cfg.M, cfg.Mp
 
     def close(self):
-        if self.ctx:
+        if self.ctx and self._owned:
             self.lib.pf_ctx_destroy(self.ctx)
-            self.ctx = None
+        self.ctx = None
 
     def __del__(self):
         try:
@@ -404,6 +415,10 @@ class Pipe:
     def vel_nonlinear(self):
         _check(self.lib.pf_vel_nonlinear(self.ctx))
 
+    def vel_transform_nonlinear(self):
+        """vel_transform + vel_nonlinear fused; vel_r..vel_curlz are not updated."""
+        _check(self.lib.pf_vel_transform_nonlinear(self.ctx))
+
     def vel_predictor(self):
         _check(self.lib.pf_vel_predictor(self.ctx))
 
@@ -474,3 +489,51 @@ class Pipe:
             _check(self.lib.pf_prof_read(self.ctx, i, C.byref(ms), C.byref(n)))
             out[name] = (ms.value, n.value)
         return out
+
+
+class Batch:
+    """Independent pipes of uneven size advanced together (pf_batch_*): one
+    CUDA graph per batch timestep, one kernel chain per pipe."""
+
+    def __init__(self, cfgs, device: int = -1):
+        self.lib = L.load()
+        arr = (L.pf_config * len(cfgs))()
+        keep = []
+        for i, cfg in enumerate(cfgs):
+            c = cfg_struct(cfg)
+            keep.append(c._r)
+            arr[i] = c
+        h = C.c_void_p()
+        self.h = None
+        _check(self.lib.pf_batch_create(len(cfgs), arr, device, C.byref(h)))
+        self.h = h
+        self.pipes = []
+        for i, cfg in enumerate(cfgs):
+            ph = C.c_void_p()
+            _check(self.lib.pf_batch_pipe(self.h, i, C.byref(ph)))
+            self.pipes.append(Pipe(cfg, _handle=ph))
+
+    def matrices(self):
+        _check(self.lib.pf_batch_matrices(self.h))
+
+    def step(self, nsteps: int = 1, orbit: bool = False) -> int:
+        """Advance every pipe; returns the corrector passes summed over pipes and steps."""
+        n = C.c_longlong()
+        _check(self.lib.pf_batch_step(self.h, nsteps, int(orbit), C.byref(n)))
+        return n.value
+
+    def sync(self):
+        _check(self.lib.pf_batch_sync(self.h))
+
+    def close(self):
+        if self.h:
+            for p in self.pipes:
+                p.ctx = None
+            self.lib.pf_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,136 @@
+"""Batched pipes (pf_batch_*) and the mixed-precision transform path.
+
+A batch runs every pipe's own kernel chain, so a pipe's state after any
+number of batched steps must equal, bit for bit, the same pipe stepped alone.
+Mixed precision (FP32 transforms and u x curl(u); FP64 elsewhere, including
+the k=m=0 mode) is held to the 1e-6 relative-L2 budget against FP64.
+"""
+import numpy as np
+import pytest
+
+import pipeflow_oracle as O
+from _util import CFG1, state_from_dev
+
+pytestmark = pytest.mark.gpu
+
+UNEVEN = [
+    dict(N=32, K=16, M=12, Mp=1, Re=1800.0, alpha=0.8, dt=0.01),
+    dict(N=48, K=32, M=24, Mp=1, Re=2400.0, alpha=1.1, dt=0.01),
+    dict(N=64, K=16, M=32, Mp=1, Re=3000.0, alpha=1.6, dt=0.01),
+    dict(N=32, K=64, M=12, Mp=2, Re=2000.0, alpha=1.3, dt=0.01),
+]
+
+
+def _cfgs(prec=0):
+    import pipeflow as P
+    return [P.PipeConfig(**d, precision=prec) for d in UNEVEN]
+
+
+def _seed(pipe, i):
+    import pipeflow as P
+    P.seeded_state(pipe, 100 + i, 1e-3)
+
+
+@pytest.mark.parametrize("orbit", [False, True], ids=["main", "orbit"])
+def test_batch_equals_lone_pipes(orbit):
+    import pipeflow as P
+    cfgs = _cfgs()
+    batch = P.Batch(cfgs)
+    batch.matrices()
+    alone = [P.Pipe(c) for c in cfgs]
+    for i, (bp, ap) in enumerate(zip(batch.pipes, alone)):
+        ap.vel_matrices()
+        _seed(bp, i)
+        _seed(ap, i)
+    nsteps = 5
+    batch.step(nsteps, orbit=orbit)
+    for ap in alone:
+        if orbit:
+            ap.steporbit(nsteps)
+        else:
+            for _ in range(nsteps):
+                ap.timestep()
+    for bp, ap in zip(batch.pipes, alone):
+        for (br, bi), (ar, ai) in zip(bp.get_state(), ap.get_state()):
+            assert np.array_equal(br, ar) and np.array_equal(bi, ai)
+        assert bp.tim.step == ap.tim.step == nsteps
+    batch.close()
+
+
+def test_batch_state_matches_oracle():
+    import pipeflow as P
+    d = UNEVEN[0]
+    batch = P.Batch([P.PipeConfig(**d)] * 2)
+    batch.matrices()
+    o = O.Pipe(O.PipeConfig(**d))
+    o.vel_matrices()
+    st = O.seeded_state(o, 5, 1e-3)
+    o.set_state(*st)
+    for bp in batch.pipes:
+        bp.set_state(*[(c.re, c.im) for c in st])
+    batch.step(4)
+    for _ in range(4):
+        o.timestep()
+    for bp in batch.pipes:
+        assert O.rel_l2(state_from_dev(bp), o.state()) <= 1e-12
+    batch.close()
+
+
+def _err_report(gm, g64):
+    s_m, s_64 = state_from_dev(gm), state_from_dev(g64)
+    err = O.rel_l2(s_m, s_64)
+    e_m, e_64 = gm.energy(), g64.energy()
+    f_m, f_64 = gm.friction()[2], g64.friction()[2]
+    return err, abs(e_m - e_64) / e_64, abs(f_m - f_64) / f_64
+
+
+def test_mixed_precision_error_budget():
+    import pipeflow as P
+    g64 = P.Pipe(P.PipeConfig(**CFG1))
+    gm = P.Pipe(P.PipeConfig(**CFG1, precision=P.PF_PREC_MIXED))
+    for g in (g64, gm):
+        g.vel_matrices()
+        P.seeded_state(g, 1, 1e-3)
+    report = {}
+    done = 0
+    for target in (1, 100):
+        while done < target:
+            g64.timestep()
+            gm.timestep()
+            done += 1
+        report[target] = _err_report(gm, g64)
+    # state rel-L2, kinetic energy and friction-velocity errors vs FP64
+    assert report[1][0] < 1e-6, report
+    assert report[100][0] < 1e-6, report
+    assert report[100][1] < 1e-6 and report[100][2] < 1e-6, report
+
+
+def test_mixed_precision_mean_mode_is_fp64():
+    """The k=m=0 nonlinear term is computed in FP64 in the mixed path."""
+    import pipeflow as P
+    g64 = P.Pipe(P.PipeConfig(**CFG1))
+    gm = P.Pipe(P.PipeConfig(**CFG1, precision=P.PF_PREC_MIXED))
+    for g in (g64, gm):
+        P.seeded_state(g, 2, 1e-3)
+        g.vel_transform_nonlinear()
+    for c in (3, 4, 5):
+        n64, nm = g64.vel_field(c).download(), gm.vel_field(c).download()
+        scale = np.abs(n64[0]).max() + np.abs(n64[1]).max()
+        # the mode-0 column agrees to FP64 rounding, the rest to FP32 accuracy
+        assert np.max(np.abs(nm[0][:, 0] - n64[0][:, 0])) <= 1e-12 * scale
+        rest = max(np.abs(nm[0][:, 1:] - n64[0][:, 1:]).max(), np.abs(nm[1][:, 1:] - n64[1][:, 1:]).max())
+        assert 0 < rest < 1e-5 * scale
+
+
+def test_fused_transform_nonlinear_matches_oracle():
+    import pipeflow as P
+    from _util import from_dev, oracle_pipe, rel_coll, state_to_dev
+    o, g = oracle_pipe(CFG1), P.Pipe(P.PipeConfig(**CFG1))
+    st = O.seeded_state(o, 3, 1e-3)
+    o.set_state(*st)
+    state_to_dev(g, st)
+    o.vel_transform()
+    o.vel_nonlinear()
+    g.vel_transform_nonlinear()
+    for i, ref in enumerate((o.vel_Nr, o.vel_Nt, o.vel_Nz)):
+        assert rel_coll(from_dev(g.vel_field(3 + i)), ref) < 1e-12
