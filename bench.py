@@ -2,16 +2,23 @@
 """Timestep throughput of the B200 pipe-flow hot path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload cfg2|cfg1] [--spinup S]
+                    [--workload batched|cfg2|cfg1]
 
-Workload (default cfg2): the larger plain FP64 drop-in case, N=64 radial
-points, K=128 axial and M=48 azimuthal modes, Mp=2, Re=5300, alpha=0.5,
-dt=0.005, seeded Hagen-Poiseuille + solenoidal perturbation at 0.1 of the
-laminar energy, spun up S (=500) steps before timing.  A "step" is one pass of
-the main.f90 loop body: nonlinear terms, predictor, corrector iterated to
-convergence.  Multi-GPU runs are independent replicas (one pipe per rank,
-seed offset by rank, no collective on the data path); the only collectives
-are the barrier and the max-over-ranks of the timed duration.
+Default workload ("batched"): 64 independent pipes with sizes drawn by
+numpy default_rng(3) uniformly from N in {32,48,64}, K in {16,32,64},
+M in {12,24,32}, Re uniform in [1800,3000], alpha uniform in [0.8,1.6],
+Mp=1, dt=0.01, each seeded (seeds 1000+) with a solenoidal perturbation at
+1e-3 of the laminar energy, run in mixed precision (FP32 transforms and
+u x curl(u), FP64 elsewhere) as one CUDA graph per batch timestep.  A "step"
+is one pass of the main.f90 loop body for every pipe (nonlinear terms,
+predictor, corrector iterated to convergence per pipe); `value` counts
+pipe-timesteps per second.  The line also reports the plain FP64 drop-in
+(the same pipes stepped one at a time) and the single large pipe N=64,
+K=128, M=48, Mp=2, Re=5300, alpha=0.5, dt=0.005 in FP64.
+
+Multi-GPU runs are independent replicas (one batch per rank, seeds offset
+by rank, no collective on the data path); the only collectives are the
+barrier and the max over ranks of the timed duration.
 
 --impl reference times the CPU restatement of the reference's step (the FP64
 oracle; the Fortran reference has no compiler on this image) on a bounded
@@ -30,20 +37,36 @@ import threading
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "softx-d-17-00015_b200"))
 
 METRIC = "batched timesteps/s vs plain at ≤1e-6 rel-L2 vs FP64; serve p50/p99 latency"
-WORKLOADS = {
+PHYS = ("N", "K", "M", "Mp", "Re", "alpha", "dt")
+SINGLE = {
     "cfg2": dict(N=64, K=128, M=48, Mp=2, Re=5300.0, alpha=0.5, dt=0.005, energy=0.1, seed=2, spinup=500),
     "cfg1": dict(N=40, K=24, M=16, Mp=1, Re=2000.0, alpha=1.25, dt=0.01, energy=1e-3, seed=1, spinup=0),
 }
-PHYS = ("N", "K", "M", "Mp", "Re", "alpha", "dt")
 
 
-def coll_bytes(w):
-    H = (2 * w["K"] - 1) * w["M"] - (w["K"] - 1)
-    return w["N"] * H * 16  # one FP64 complex coll field, S
+def batched_configs(npipes: int = 64, seed: int = 3):
+    """The uneven pipe mix of the batched workload (sizes, Re, alpha)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(npipes):
+        out.append(dict(N=int(rng.choice([32, 48, 64])), K=int(rng.choice([16, 32, 64])),
+                        M=int(rng.choice([12, 24, 32])), Mp=1, Re=float(rng.uniform(1800, 3000)),
+                        alpha=float(rng.uniform(0.8, 1.6)), dt=0.01))
+    return out
+
+
+def harmonics_count(d):
+    return (2 * d["K"] - 1) * d["M"] - (d["K"] - 1)
+
+
+def coll_bytes(d):
+    return d["N"] * harmonics_count(d) * 16  # one FP64 complex coll field, S
 
 
 def peaks():
@@ -98,86 +121,152 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def cpu_baseline(w, nsteps: int):
-    """Time the FP64 oracle (CPU restatement of the reference step)."""
+def cpu_baseline(workload: str, nsample: int):
+    """Time the FP64 oracle (CPU restatement of the reference step) on a
+    bounded sample of the workload: one step of each of the first `nsample`
+    pipes (batched) or `nsample` steps of the single pipe."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import pipeflow_oracle as O
+    if workload == "batched":
+        cfgs = batched_configs()[:nsample]
+        pipes = []
+        for i, d in enumerate(cfgs):
+            o = O.Pipe(O.PipeConfig(**d))
+            o.vel_matrices()
+            o.set_state(*O.seeded_state(o, 1000 + i, 1e-3))
+            pipes.append(o)
+        t0 = time.perf_counter()
+        for o in pipes:
+            o.timestep()
+        dt = time.perf_counter() - t0
+        return {"value": len(pipes) / dt, "unit": "timesteps/s", "cores": 1, "kind": "port",
+                "sample": f"one main-loop step of each of the first {len(pipes)} pipes of the 64-pipe mix, "
+                          f"FP64 numpy/scipy oracle, after matrices and seeding"}
+    w = SINGLE[workload]
     o = O.Pipe(O.PipeConfig(**{k: w[k] for k in PHYS}))
     o.vel_matrices()
     o.set_state(*O.seeded_state(o, w["seed"], w["energy"]))
-    o.timestep()  # untimed warm-up
+    o.timestep()
     t0 = time.perf_counter()
-    for _ in range(nsteps):
+    for _ in range(nsample):
         o.timestep()
     dt = time.perf_counter() - t0
-    return {"value": nsteps / dt, "unit": "timesteps/s", "cores": 1, "kind": "port",
-            "sample": f"{nsteps} steps of the FP64 numpy/scipy oracle on the same workload "
+    return {"value": nsample / dt, "unit": "timesteps/s", "cores": 1, "kind": "port",
+            "sample": f"{nsample} steps of the FP64 numpy/scipy oracle on the same pipe "
                       f"(after matrices, seed and 1 warm-up step; no spin-up)"}
 
 
-def run_reference(args, w, rank):
+def read_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == workload and parts[1] == kernel:
+            try:
+                return float(parts[2])
+            except ValueError:
+                return None
+    return None
+
+
+# algorithmic bytes of one launch of each kernel category, in units of the
+# coll field size S: the coll fields it must read and write once (factors,
+# twiddles and transform scratch are not algorithmic)
+PER_LAUNCH_S = {"lusolve": 2, "stencil": 2, "ew": 2, "infl": 4, "zinv": 3, "thinv": 3, "thfwd": 3,
+                "zfwd": 3, "step": 10, "factor": 0}
+
+
+def config_of(args, w=None):
+    if args.workload == "batched":
+        cfgs = batched_configs(args.pipes)
+        return {"workload": f"batched: {args.pipes} uneven pipes (N in 32/48/64, K in 16/32/64, M in 12/24/32, "
+                            f"Re 1800-3000, alpha 0.8-1.6, dt=0.01) in mixed precision, one CUDA graph per "
+                            f"batch step, corrector to convergence per pipe",
+                "pipes_per_gpu": args.pipes, "precision": "mixed (FP32 transforms, FP64 solves)",
+                "sum_H": sum(harmonics_count(d) for d in cfgs), "parallelism": f"replicas x{args.gpus}",
+                "l2": "working set of 64 pipes (~1-2 GB) larger than the 126 MB L2; no flush"}
+    return {"workload": f"{args.workload}: plain FP64 drop-in, N={w['N']} K={w['K']} M={w['M']} Mp={w['Mp']} "
+                        f"Re={w['Re']} alpha={w['alpha']} dt={w['dt']}, seeded perturbation E={w['energy']} E_lam, "
+                        f"spin-up {w['spinup']} steps",
+            "N": w["N"], "K": w["K"], "M": w["M"], "Mp": w["Mp"], "H": harmonics_count(w), "Re": w["Re"],
+            "alpha": w["alpha"], "dt": w["dt"], "pipes_per_gpu": 1, "parallelism": f"replicas x{args.gpus}",
+            "l2": "working set (~0.7 GB) larger than the 126 MB L2; no flush"}
+
+
+def run_reference(args, rank):
     if rank != 0:
         return
-    nsteps = max(1, min(args.steps, args.ref_steps))
-    base = cpu_baseline(w, nsteps)
+    nsample = max(1, min(args.steps, args.ref_steps))
+    base = cpu_baseline(args.workload, nsample)
+    w = SINGLE.get(args.workload)
     line = {
         "impl": "reference", "metric": METRIC, "value": base["value"], "unit": "timesteps/s",
-        "n_gpus": args.gpus, "steps": nsteps, "warmup": 1, "ms_per_step": 1e3 / base["value"],
+        "n_gpus": args.gpus, "steps": nsample, "warmup": 1, "ms_per_step": 1e3 / base["value"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": config_of(args, w),
-        "cpu_baseline": base,
+        "data": "synthetic", "config": config_of(args, w), "cpu_baseline": base,
         "e2e": {"value": base["value"], "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def config_of(args, w):
-    H = (2 * w["K"] - 1) * w["M"] - (w["K"] - 1)
-    return {"workload": f"{args.workload}: plain FP64 drop-in, N={w['N']} K={w['K']} M={w['M']} Mp={w['Mp']} "
-                        f"Re={w['Re']} alpha={w['alpha']} dt={w['dt']}, seeded perturbation E={w['energy']} E_lam, "
-                        f"spin-up {w['spinup']} steps",
-            "N": w["N"], "K": w["K"], "M": w["M"], "Mp": w["Mp"], "H": H, "Re": w["Re"], "alpha": w["alpha"],
-            "dt": w["dt"], "pipes_per_gpu": 1, "parallelism": f"replicas x{args.gpus}",
-            "l2": "working set (~0.7 GB) larger than the 126 MB L2; no flush"}
+def dev_timer(torch, stream):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    return e0, e1
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
-    ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=list(WORKLOADS))
-    ap.add_argument("--spinup", type=int, default=None)
-    ap.add_argument("--ref-steps", type=int, default=3)
-    ap.add_argument("--e2e-steps", type=int, default=50)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    args = ap.parse_args()
-    args.warmup = max(3, args.warmup)
-    w = dict(WORKLOADS[args.workload])
+def plain_sequential(P, torch, cfgs, seeds, steps=3):
+    """The plain FP64 drop-in on the same pipes, one pipe at a time."""
+    total_ms, total_steps = 0.0, 0
+    stream = torch.cuda.Stream()
+    for d, sd in zip(cfgs, seeds):
+        p = P.Pipe(P.PipeConfig(**d))
+        p.lib.pf_ctx_set_stream(p.ctx, stream.cuda_stream)
+        p.vel_matrices()
+        P.seeded_state(p, sd, 1e-3)
+        for _ in range(3):  # eager step + both graph parities captured
+            p.timestep()
+        e0, e1 = dev_timer(torch, stream)
+        e0.record(stream)
+        for _ in range(steps):
+            p.timestep()
+        e1.record(stream)
+        stream.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        total_steps += steps
+        p.close()
+    return total_steps / (total_ms / 1e3), total_ms / total_steps
+
+
+def mixed_error(P, d, seed, nsteps=100):
+    """State rel-L2, kinetic-energy and friction errors of the mixed path
+    against FP64 on one pipe of the mix after nsteps."""
+    g64 = P.Pipe(P.PipeConfig(**d))
+    gm = P.Pipe(P.PipeConfig(**d, precision=P.PF_PREC_MIXED))
+    for g in (g64, gm):
+        g.vel_matrices()
+        P.seeded_state(g, seed, 1e-3)
+        for _ in range(nsteps):
+            g.timestep()
+    num = den = 0.0
+    for (ar, ai), (br, bi) in zip(gm.get_state(), g64.get_state()):
+        num += float(np.sum((ar - br) ** 2 + (ai - bi) ** 2))
+        den += float(np.sum(br ** 2 + bi ** 2))
+    e64, em = g64.energy(), gm.energy()
+    f64, fm = g64.friction()[2], gm.friction()[2]
+    out = {"steps": nsteps, "pipe": d, "state_rel_l2": math.sqrt(num / den),
+           "energy_rel": abs(em - e64) / e64, "friction_rel": abs(fm - f64) / f64}
+    g64.close()
+    gm.close()
+    return out
+
+
+def run_single(args, torch, P, dist, world, rank, local):
+    """One large FP64 pipe per rank (cfg2 / cfg1)."""
+    w = dict(SINGLE[args.workload])
     if args.spinup is not None:
         w["spinup"] = args.spinup
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-
-    if args.impl == "reference":
-        run_reference(args, w, rank)
-        return
-
-    import torch
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(local)
-    import pipeflow as P
-
     pipe = P.Pipe(P.PipeConfig(**{k: w[k] for k in PHYS}), device=local)
     stream = torch.cuda.Stream()
     pipe.lib.pf_ctx_set_stream(pipe.ctx, stream.cuda_stream)
@@ -186,7 +275,6 @@ def main():
     with torch.cuda.stream(stream):
         for _ in range(w["spinup"]):
             pipe.timestep()
-        # warm-up with every kernel category timed to find the dominant one
         pipe.prof_enable(True)
         for _ in range(args.warmup):
             pipe.timestep()
@@ -203,7 +291,7 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
         n0 = pipe.launches()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0, ev1 = dev_timer(torch, stream)
         ncorr = 0
         with ClockSampler(local) as clk:
             ev0.record(stream)
@@ -211,21 +299,17 @@ def main():
                 ncorr += pipe.timestep()
             ev1.record(stream)
             stream.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
         launches = pipe.launches() - n0
         ms = ev0.elapsed_time(ev1)
         dom_ms, dom_n = pipe.prof_read()[dom]
         pipe.prof_enable(False)
-
         # end to end through the C ABI with pinned host buffers
         N, H = pipe.N, pipe.H
         host = [torch.empty((H, N), dtype=torch.float64, pin_memory=True) for _ in range(6)]
         ptrs = [P.api.C.cast(t.data_ptr(), P._lib.DP) for t in host]
         P.api._check(pipe.lib.pf_vel_get_state(pipe.ctx, *ptrs))
         ne = max(1, min(args.e2e_steps, args.steps))
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0, e1 = dev_timer(torch, stream)
         e0.record(stream)
         for _ in range(ne):
             P.api._check(pipe.lib.pf_vel_set_state(pipe.ctx, *ptrs))
@@ -234,67 +318,181 @@ def main():
         e1.record(stream)
         stream.synchronize()
         e2e_ms = e0.elapsed_time(e1)
+    pipe.close()
+    S = coll_bytes(w)
+    nc = ncorr / args.steps
+    per_launch = PER_LAUNCH_S[dom] * S
+    res = dict(ms=ms, e2e_ms=e2e_ms, ne=ne, count=1, launches=launches, clk=clk.summary(),
+               extra={"corrector_iterations_per_step": nc,
+                      "algorithmic_bytes_per_step": S * (15 + 21 * nc),
+                      "step_bandwidth_gbs": S * (15 + 21 * nc) / (ms / args.steps / 1e3) / 1e9},
+               dom=dom, dom_ms=dom_ms, dom_n=dom_n, per_launch=per_launch,
+               h2d=6 * N * H * 8, d2h=6 * N * H * 8, dtype="f64", config=config_of(args, w))
+    return res
 
+
+def run_batched(args, torch, P, dist, world, rank, local):
+    """One batch of uneven mixed-precision pipes per rank."""
+    cfgs = batched_configs(args.pipes)
+    seeds = [1000 + rank * args.pipes + i for i in range(args.pipes)]
+    batch = P.Batch([P.PipeConfig(**d, precision=P.PF_PREC_MIXED) for d in cfgs], device=local)
+    batch.matrices()
+    for p, sd in zip(batch.pipes, seeds):
+        P.seeded_state(p, sd, 1e-3)
+    h = P.api.C.c_void_p()
+    P.api._check(batch.lib.pf_batch_stream(batch.h, P.api.C.byref(h)))
+    master = torch.cuda.ExternalStream(h.value)
+    batch.step(args.spinup if args.spinup is not None else 20)
+    batch.prof_enable(True)
+    batch.step(args.warmup)
+    prof = batch.prof_read()
+    dom = max(prof, key=lambda k: prof[k][0])
+    batch.prof_enable([dom])
+    batch.step(2)  # re-capture both parities with the dominant category's event nodes
+    batch.prof_enable([dom])
+    batch.sync()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    n0 = sum(p.launches() for p in batch.pipes)
+    ev0, ev1 = dev_timer(torch, master)
+    with ClockSampler(local) as clk:
+        ev0.record(master)
+        passes = batch.step(args.steps)
+        ev1.record(master)
+        master.synchronize()
+    launches = sum(p.launches() for p in batch.pipes) - n0
+    ms = ev0.elapsed_time(ev1)
+    dom_ms, dom_n = batch.prof_read()[dom]
+    batch.prof_enable(False)
+    # end to end through the C ABI: every pipe's state from pinned host
+    # memory in, one batch step, every state back out
+    host = []
+    for p in batch.pipes:
+        bufs = [torch.empty((p.H, p.N), dtype=torch.float64, pin_memory=True) for _ in range(6)]
+        ptrs = [P.api.C.cast(t.data_ptr(), P._lib.DP) for t in bufs]
+        P.api._check(p.lib.pf_vel_get_state(p.ctx, *ptrs))
+        host.append((bufs, ptrs))
+    ne = max(1, min(args.e2e_steps, args.steps))
+    e0, e1 = dev_timer(torch, master)
+    e0.record(master)
+    for _ in range(ne):
+        for p, (_, ptrs) in zip(batch.pipes, host):
+            P.api._check(p.lib.pf_vel_set_state(p.ctx, *ptrs))
+        batch.step(1)
+        for p, (_, ptrs) in zip(batch.pipes, host):
+            P.api._check(p.lib.pf_vel_get_state(p.ctx, *ptrs))
+    e1.record(master)
+    master.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    batch.close()
+    S = [coll_bytes(d) for d in cfgs]
+    nc = passes / (args.steps * args.pipes)
+    step_bytes = sum(s * (15 + 21 * nc) for s in S)
+    # dominant category: algorithmic bytes per launch averaged over the pipes
+    per_launch = PER_LAUNCH_S[dom] * sum(S) / len(S)
+    io = sum(6 * d["N"] * harmonics_count(d) * 8 for d in cfgs)
+    extra = {"corrector_iterations_per_step": nc, "algorithmic_bytes_per_batch_step": step_bytes,
+             "batch_step_ms": ms / args.steps,
+             "step_roofline": {"bound": "hbm", "scope": "whole batch step (all stages, all pipes)",
+                               "achieved": step_bytes / (ms / args.steps / 1e3) / 1e9, "unit": "GB/s"}}
+    if rank == 0:
+        plain, plain_ms = plain_sequential(P, torch, cfgs[:args.plain_pipes], seeds[:args.plain_pipes])
+        extra["plain"] = {"value": plain, "unit": "timesteps/s", "ms_per_pipe_step": plain_ms,
+                          "what": f"the same pipes (first {args.plain_pipes}) in FP64, one pipe at a time "
+                                  f"through pf_timestep"}
+        extra["batched_over_plain"] = (args.pipes * args.steps / (ms / 1e3)) / plain
+        extra["mixed_vs_fp64"] = mixed_error(P, cfgs[0], seeds[0], args.err_steps)
+        if args.with_cfg2:
+            sub = argparse.Namespace(**vars(args))
+            sub.workload, sub.spinup, sub.steps = "cfg2", args.cfg2_spinup, args.cfg2_steps
+            r = run_single(sub, torch, P, None, 1, 0, local)
+            extra["plain_cfg2"] = {"value": sub.steps / (r["ms"] / 1e3), "unit": "timesteps/s",
+                                   "ms_per_step": r["ms"] / sub.steps, "workload": r["config"]["workload"],
+                                   "dominant_kernel": r["dom"],
+                                   "dominant_avg_launch_us": r["dom_ms"] * 1e3 / max(r["dom_n"], 1),
+                                   **r["extra"]}
+    return dict(ms=ms, e2e_ms=e2e_ms, ne=ne, count=args.pipes, launches=launches, clk=clk.summary(),
+                extra=extra, dom=dom, dom_ms=dom_ms, dom_n=dom_n, per_launch=per_launch, h2d=io, d2h=io,
+                dtype="mixed: f32 transforms, f64 solves", config=config_of(args))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "cfg2", "cfg1"])
+    ap.add_argument("--pipes", type=int, default=64)
+    ap.add_argument("--spinup", type=int, default=None)
+    ap.add_argument("--ref-steps", type=int, default=4)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--plain-pipes", type=int, default=64)
+    ap.add_argument("--err-steps", type=int, default=100)
+    ap.add_argument("--cfg2-spinup", type=int, default=50)
+    ap.add_argument("--cfg2-steps", type=int, default=200)
+    ap.add_argument("--no-cfg2", dest="with_cfg2", action="store_false")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    dist = None
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    import pipeflow as P
+
+    run = run_batched if args.workload == "batched" else run_single
+    r = run(args, torch, P, dist, world, rank, local)
+    ms, e2e_ms = r["ms"], r["e2e_ms"]
     if dist:
         t = torch.tensor([ms, e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, e2e_ms = float(t[0]), float(t[1])
-    value = world * args.steps / (ms / 1e3)
-    e2e_value = world * ne / (e2e_ms / 1e3)
+    value = world * r["count"] * args.steps / (ms / 1e3)
+    e2e_value = world * r["count"] * r["ne"] / (e2e_ms / 1e3)
 
     if rank == 0:
-        S = coll_bytes(w)
         peak, src = peaks()
-        # algorithmic bytes of one launch of the dominant category: the coll
-        # fields it must read and write once (factors, twiddles, FFT scratch
-        # are not algorithmic)
-        per_launch = {"lusolve": 2 * S, "stencil": 2 * S, "ew": 2 * S, "infl": 4 * S,
-                      "zinv": 3 * S, "thinv": 3 * S, "thfwd": 3 * S, "zfwd": 3 * S, "step": 12 * S,
-                      "factor": 0}[dom]
-        avg_launch_s = (dom_ms / 1e3) / max(dom_n, 1)
-        achieved = per_launch / avg_launch_s / 1e9 if avg_launch_s > 0 else None
-        traffic = read_traffic(dom, args.workload)
+        avg_launch_s = (r["dom_ms"] / 1e3) / max(r["dom_n"], 1)
+        achieved = r["per_launch"] / avg_launch_s / 1e9 if avg_launch_s > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_of(args, w),
-            "corrector_iterations_per_step": ncorr / args.steps,
-            "algorithmic_bytes_per_step": S * (15 + 21 * ncorr / args.steps),
-            "step_bandwidth_gbs": S * (15 + 21 * ncorr / args.steps) / (ms / args.steps / 1e3) / 1e9,
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                         "peak_source": src, "unit": "GB/s",
-                         "frac": achieved / peak if achieved else None,
-                         "algorithmic_bytes_per_launch": per_launch,
-                         "avg_launch_us": avg_launch_s * 1e6, "launches": dom_n,
-                         "traffic": traffic},
-            "gpu_launches": launches,
-            "e2e": {"value": e2e_value, "unit": "timesteps/s", "steps": ne,
-                    "h2d_bytes_per_step": 6 * N * H * 8, "d2h_bytes_per_step": 6 * N * H * 8},
-            "clocks": clk.summary(),
+            "scaling": "weak", "vs_baseline": None, "dtype": r["dtype"], "data": "synthetic",
+            "config": r["config"],
+            "roofline": {"bound": "hbm", "kernel": r["dom"], "achieved": achieved, "peak": peak,
+                         "peak_source": src, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                         "algorithmic_bytes_per_launch": r["per_launch"],
+                         "avg_launch_us": avg_launch_s * 1e6, "launches": r["dom_n"],
+                         "traffic": read_traffic(r["dom"], args.workload)},
+            "gpu_launches": r["launches"],
+            "e2e": {"value": e2e_value, "unit": "timesteps/s", "steps": r["ne"],
+                    "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+            "clocks": r["clk"],
         }
+        if args.workload == "batched":
+            line["roofline"]["note"] = ("kernel spans of concurrent pipes overlap in time, so the per-launch "
+                                        "duration includes GPU sharing and frac is a lower bound")
+        line.update(r["extra"])
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(w, max(1, args.ref_steps))
+            line["cpu_baseline"] = cpu_baseline(args.workload, max(1, args.ref_steps))
         print(json.dumps(line), flush=True)
-    pipe.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-
-
-def read_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch from the committed ncu summary, if present."""
-    p = ROOT / "profiles" / "traffic.txt"
-    if not p.exists():
-        return None
-    for line in p.read_text().splitlines():
-        parts = line.split()
-        if len(parts) >= 3 and parts[0] == workload and parts[1] == kernel:
-            try:
-                return float(parts[2])
-            except ValueError:
-                return None
-    return None
 
 
 if __name__ == "__main__":

@@ -242,6 +242,13 @@ int pf_batch_matrices(pf_batch *b);
  * (may be NULL) = corrector passes summed over pipes and steps. */
 int pf_batch_step(pf_batch *b, int nsteps, int orbit, long long *corr_passes);
 int pf_batch_sync(pf_batch *b);
+/* The cudaStream_t the batch's graphs are launched on (for event timing). */
+int pf_batch_stream(pf_batch *b, void **stream);
+/* Kernel-category event timing for every pipe (see pf_prof_enable), and the
+ * totals summed over the pipes.  Kernel spans of different pipes overlap in
+ * time, so per-launch durations here include the sharing of the GPU. */
+int pf_batch_prof_enable(pf_batch *b, int mask);
+int pf_batch_prof_read(pf_batch *b, int cat, double *ms, unsigned long long *launches);
 
 /* ------------------------------------------------------- instrumentation */
 /* Kernel categories timed by CUDA events when profiling is on (the reference

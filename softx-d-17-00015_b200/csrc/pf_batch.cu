@@ -28,13 +28,33 @@ struct pf_batch {
     int parity;
     bool warm;
     DevScalars *hsc;           // pinned, one per pipe
+    // event pairs of profiled categories captured into each graph:
+    // (pipe, category, start, stop)
+    struct Ev {
+        int pipe, cat;
+        cudaEvent_t a, b;
+    };
+    std::vector<Ev> gev[2][2];
+    std::vector<unsigned long long> gnp[2][2];  // kernels per pipe in each graph
 };
 
-static void batch_free(pf_batch *b) {
+// Destroy the batch graphs and hand their event pairs back to the pipes.
+static void batch_graphs_reset(pf_batch *b) {
     if (b->master) cudaStreamSynchronize(b->master);
     for (int o = 0; o < 2; ++o)
-        for (int p = 0; p < 2; ++p)
+        for (int p = 0; p < 2; ++p) {
             if (b->g[o][p]) cudaGraphExecDestroy(b->g[o][p]);
+            b->g[o][p] = nullptr;
+            for (auto &e : b->gev[o][p]) {
+                b->pipes[e.pipe]->ev_pool.push_back(e.a);
+                b->pipes[e.pipe]->ev_pool.push_back(e.b);
+            }
+            b->gev[o][p].clear();
+        }
+}
+
+static void batch_free(pf_batch *b) {
+    if (!b->pipes.empty()) batch_graphs_reset(b);
     for (cudaEvent_t e : b->join) cudaEventDestroy(e);
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->master) cudaStreamDestroy(b->master);
@@ -89,13 +109,8 @@ extern "C" int pf_batch_pipe(pf_batch *b, int i, pf_ctx **out) {
 
 extern "C" int pf_batch_matrices(pf_batch *b) {
     PF_ARG(b, "null batch");
+    batch_graphs_reset(b);
     for (pf_ctx *c : b->pipes) PF_TRY(pf_vel_matrices(c));
-    for (int o = 0; o < 2; ++o)
-        for (int p = 0; p < 2; ++p)
-            if (b->g[o][p]) {
-                cudaGraphExecDestroy(b->g[o][p]);
-                b->g[o][p] = nullptr;
-            }
     return PF_OK;
 }
 
@@ -117,9 +132,12 @@ static int pipe_body(pf_ctx *c, int orbit) {
     return PF_OK;
 }
 
-static int batch_capture(pf_batch *b, int orbit, cudaGraphExec_t *exec, unsigned long long *nk) {
-    unsigned long long n0 = 0;
-    for (pf_ctx *c : b->pipes) n0 += c->launches;
+static int batch_capture(pf_batch *b, int orbit, int par, cudaGraphExec_t *exec, unsigned long long *nk) {
+    std::vector<unsigned long long> n0(b->n);
+    for (int i = 0; i < b->n; ++i) n0[i] = b->pipes[i]->launches;
+    std::vector<size_t> open0((size_t)b->n * PF_K_NCAT);
+    for (int i = 0; i < b->n; ++i)
+        for (int c = 0; c < PF_K_NCAT; ++c) open0[(size_t)i * PF_K_NCAT + c] = b->pipes[i]->ev_open[c].size();
     cudaGraph_t graph = nullptr;
     PF_CUDA(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
     int s = PF_OK;
@@ -135,6 +153,14 @@ static int batch_capture(pf_batch *b, int orbit, cudaGraphExec_t *exec, unsigned
             s = PF_ERR_CUDA;
     }
     const cudaError_t e = cudaStreamEndCapture(b->master, &graph);
+    // event pairs recorded during the capture belong to the graph
+    for (int i = 0; i < b->n; ++i)
+        for (int c = 0; c < PF_K_NCAT; ++c) {
+            auto &open = b->pipes[i]->ev_open[c];
+            const size_t from = open0[(size_t)i * PF_K_NCAT + c];
+            for (size_t k = from; k < open.size(); ++k) b->gev[orbit][par].push_back({i, c, open[k].first, open[k].second});
+            open.resize(from);
+        }
     // the capture swapped each pipe's host pointers; the replay does it for real
     for (pf_ctx *c : b->pipes)
         for (int i = 0; i < 3; ++i) std::swap(c->vel[i].d, c->prev[i].d);
@@ -150,10 +176,14 @@ static int batch_capture(pf_batch *b, int orbit, cudaGraphExec_t *exec, unsigned
         pf_set_error("batch graph instantiation failed: %s", cudaGetErrorString(e2));
         return PF_ERR_CUDA;
     }
-    unsigned long long n1 = 0;
-    for (pf_ctx *c : b->pipes) n1 += c->launches;
-    *nk = n1 - n0;
-    for (pf_ctx *c : b->pipes) c->launches = c->launches;  // per-pipe counters keep the capture
+    // kernels per pipe are counted at each replay, not at capture
+    b->gnp[orbit][par].assign(b->n, 0);
+    *nk = 0;
+    for (int i = 0; i < b->n; ++i) {
+        b->gnp[orbit][par][i] = b->pipes[i]->launches - n0[i];
+        *nk += b->gnp[orbit][par][i];
+        b->pipes[i]->launches = n0[i];
+    }
     return PF_OK;
 }
 
@@ -189,15 +219,25 @@ extern "C" int pf_batch_step(pf_batch *b, int nsteps, int orbit, long long *corr
                 pf_set_error("pf_batch_step: pipes out of step (pointer parity differs)");
                 return PF_ERR_STATE;
             }
-        if (!b->g[orbit][p]) PF_TRY(batch_capture(b, orbit, &b->g[orbit][p], &b->gn[orbit][p]));
+        if (!b->g[orbit][p]) PF_TRY(batch_capture(b, orbit, p, &b->g[orbit][p], &b->gn[orbit][p]));
         PF_CUDA(cudaGraphLaunch(b->g[orbit][p], b->master));
         for (pf_ctx *c : b->pipes) {
             for (int i = 0; i < 3; ++i) std::swap(c->vel[i].d, c->prev[i].d);
             c->parity ^= 1;
             c->cfl_fused = true;
-            c->launches += b->gn[orbit][p] / b->n;
         }
+        for (int i = 0; i < b->n; ++i) b->pipes[i]->launches += b->gnp[orbit][p][i];
         PF_CUDA(cudaStreamSynchronize(b->master));
+        for (auto &e : b->gev[orbit][p]) {  // kernel times of the profiled categories
+            float ms = 0.f;
+            pf_ctx *c = b->pipes[e.pipe];
+            if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
+                c->prof_ms[e.cat] += ms;
+                c->prof_n[e.cat] += 1;
+            } else {
+                cudaGetLastError();
+            }
+        }
         for (int i = 0; i < b->n; ++i) {
             pf_ctx *c = b->pipes[i];
             c->tim.dterr = std::max(c->tim.dterr, std::sqrt(bits_to_double(b->hsc[i].dterr2_bits)));
@@ -228,5 +268,40 @@ extern "C" int pf_batch_sync(pf_batch *b) {
     PF_ARG(b, "null batch");
     PF_CUDA(cudaStreamSynchronize(b->master));
     for (pf_ctx *c : b->pipes) PF_CUDA(cudaStreamSynchronize(c->stream));
+    return PF_OK;
+}
+
+// Event timing of the categories in `mask` (1 << PF_K_*) for every pipe of
+// the batch, inside the batch graphs; each call clears the totals.
+extern "C" int pf_batch_prof_enable(pf_batch *b, int mask) {
+    PF_ARG(b, "null batch");
+    bool changed = false;
+    for (pf_ctx *c : b->pipes) changed |= (c->prof_mask != mask);
+    if (changed) batch_graphs_reset(b);
+    for (pf_ctx *c : b->pipes) PF_TRY(pf_prof_enable(c, mask));
+    return PF_OK;
+}
+
+// Device milliseconds and launches of category `cat` summed over the pipes.
+extern "C" int pf_batch_prof_read(pf_batch *b, int cat, double *ms, unsigned long long *launches) {
+    PF_ARG(b && cat >= 0 && cat < PF_K_NCAT, "pf_batch_prof_read: bad argument");
+    double t = 0.0;
+    unsigned long long n = 0;
+    for (pf_ctx *c : b->pipes) {
+        double m = 0.0;
+        unsigned long long k = 0;
+        PF_TRY(pf_prof_read(c, cat, &m, &k));
+        t += m;
+        n += k;
+    }
+    if (ms) *ms = t;
+    if (launches) *launches = n;
+    return PF_OK;
+}
+
+// The batch's master stream (graph launches are ordered on it).
+extern "C" int pf_batch_stream(pf_batch *b, void **stream) {
+    PF_ARG(b && stream, "pf_batch_stream: bad argument");
+    *stream = (void *)b->master;
     return PF_OK;
 }

@@ -189,7 +189,6 @@ static int ctx_init(pf_ctx *ctx, const pf_config *cfg, int device) {
     PF_TRY(pf_alloc(ctx, (void **)&ctx->red, (size_t)(3 * N + g.Hp + 64) * sizeof(double)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->cflmax, (size_t)3 * N * sizeof(unsigned long long)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->anypiv, sizeof(int)));
-    PF_TRY(pf_alloc(ctx, (void **)&ctx->LNp_pivd, (size_t)N * g.Hp * sizeof(double)));
     ctx->T_bytes = (size_t)6 * N * g.M * g.Z * sizeof(double2);
     PF_TRY(pf_alloc(ctx, &ctx->T, ctx->T_bytes));
     // LU factor storage for the four matrix sets
@@ -198,6 +197,7 @@ static int ctx_init(pf_ctx *ctx, const pf_config *cfg, int device) {
         A->ctx = ctx;
         PF_TRY(pf_alloc(ctx, (void **)&A->lu, (size_t)NLU * N * g.Hp * sizeof(double)));
         PF_TRY(pf_alloc(ctx, (void **)&A->piv, (size_t)N * g.Hp));
+        PF_TRY(pf_alloc(ctx, (void **)&A->pivd, (size_t)N * g.Hp * sizeof(double)));
     }
     ctx->Ltp.ctx = ctx->Ltm.ctx = ctx->Ltz.ctx = ctx;
     // tim_precompute (timestep.f90:29-40)

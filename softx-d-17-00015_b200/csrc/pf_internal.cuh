@@ -122,6 +122,7 @@ struct pf_lumesh {
     pf_ctx *ctx;
     int PM, BC;
     int pivoted;         // host copy: any row interchange in the factorisation
+    double *pivd;        // pivot offsets as doubles [col*Hp + nh] (context sets only)
     double c1, c2;
     double *lu;
     unsigned char *piv;
@@ -163,7 +164,6 @@ struct pf_ctx {
     unsigned long long *cflmax;  // 3*N CFL maxima of the last fused transform
     bool cfl_fused;              // cflmax is current (else use vel_r/t/z)
     int *anypiv;         // per LU set: 1 if dgbtf2 swapped any row
-    double *LNp_pivd;    // LNp pivot offsets as doubles [col*Hp + nh]
     void *T;             // FFT scratch: 6*N*M*Z complex (FP64)
     size_t T_bytes;
     int zinv_mc, zfwd_mc, th_zc;   // tile sizes

@@ -356,17 +356,26 @@ int pf_launch_flux1(pf_ctx *ctx) {
 }
 
 // ---------------------------------------------------------- vel_matrices
+__global__ void k_piv_to_double(const unsigned char *__restrict__ piv, double *__restrict__ pivd, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        pivd[i] = (double)piv[i];
+}
+
 static int lumesh_init(pf_ctx *ctx, pf_lumesh *A, int PM, int BC, double c1, double c2) {
     A->PM = PM;
     A->BC = BC;
     A->c1 = c1;
     A->c2 = c2;
-    return pf_launch_lu_factor(ctx, A);
-}
-
-__global__ void k_piv_to_double(const unsigned char *__restrict__ piv, double *__restrict__ pivd, size_t n) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        pivd[i] = (double)piv[i];
+    PF_TRY(pf_launch_lu_factor(ctx, A));
+    if (A->pivd) {  // pivots as doubles, staged by the fused solves with 8-byte copies
+        const size_t np = (size_t)ctx->g.N * ctx->g.Hp;
+        {
+            ProfScope ps_(ctx, PF_K_FACTOR);
+            k_piv_to_double<<<grid1(np, 256), 256, 0, ctx->stream>>>(A->piv, A->pivd, np);
+        }
+        PF_LAUNCHED(ctx);
+    }
+    return PF_OK;
 }
 
 // velocity.f90:120-146 including vel_adjustFlux(0) and vel_adjPPE(0)
@@ -376,12 +385,6 @@ int pf_vel_matrices_impl(pf_ctx *ctx) {
     const pf_config &cfg = ctx->cfg;
     if (!ctx->LNp_set) {
         PF_TRY(lumesh_init(ctx, &ctx->LNp, 0, 1, 0.0, 1.0));
-        const size_t np = (size_t)g.N * g.Hp;
-        {
-            ProfScope ps_(ctx, PF_K_FACTOR);
-            k_piv_to_double<<<grid1(np, 256), 256, 0, ctx->stream>>>(ctx->LNp.piv, ctx->LNp_pivd, np);
-        }
-        PF_LAUNCHED(ctx);
         ctx->LNp_set = true;
     }
     double d1 = 1.0 / ctx->tim.dt;

@@ -9,8 +9,8 @@
 //                    BC=1, mean mode zeroed; timestep.f90:102-123)
 //   S3 k_step_proj : the projection rhs - rt2pm(grad p) with zero boundary
 //                    rows (velocity.f90:232-236, 376-378)
-//   S4 k_solve_ld  : the u+, u-, uz Helmholtz solves (LDp, LDm, LDz, which
-//                    never pivot)
+//   S4 k_solve_ld  : the u+, u-, uz Helmholtz solves (LDp, LDm, LDz; the
+//                    pivot-free sweep unless that factorisation pivoted)
 //   S5 k_step_final: influence-matrix correction (velocity.f90:238-256),
 //                    pm2rt, constant-flux adjustment for k=m=0
 //                    (velocity.f90:170-175), mean-mode symmetry zeros, and the
@@ -34,6 +34,8 @@ struct StepArgs {
     double2 *u[3];         // vel_u (read as u_old by the corrector, written)
     const double *lnp, *ldp, *ldm, *ldz;
     const double *pivd;    // LNp pivots as doubles [col*Hp + nh]
+    const double *pivld[3];  // LDp/LDm/LDz pivots as doubles
+    int ldpiv[3];          // 1 if that Helmholtz factorisation pivoted
     const double *U, *Ainv, *Ui;
     DevMesh dm;
     Geo g;
@@ -319,7 +321,8 @@ __global__ void k_step_proj(StepArgs a) {
     a.rl[2][at] = make_double2(vz.x - (-pv.y * kal), vz.y - (pv.x * kal));
 }
 
-// S4: warp = one (system, re/im) of 32 consecutive modes; LD never pivots
+// S4: warp = one (system, re/im) of 32 consecutive modes; the pivot-free
+// sweep is used for the systems whose factorisation did not pivot
 __global__ void __launch_bounds__(192) k_solve_ld(StepArgs a) {
     extern __shared__ double ring4[];
     const Geo &g = a.g;
@@ -331,7 +334,10 @@ __global__ void __launch_bounds__(192) k_solve_ld(StepArgs a) {
     const double *rhs = reinterpret_cast<const double *>(a.rl[sys]) + 2 * (size_t)nh + part;
     double *out = reinterpret_cast<double *>(a.v[sys]) + 2 * (size_t)nh + part;
     const double *lu = sys == 0 ? a.ldp : sys == 1 ? a.ldm : a.ldz;
-    solve_async<false>(lu, nullptr, g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x, blockDim.x);
+    if (a.ldpiv[sys])  // pivoting band (low Re, small dt or very clustered meshes)
+        solve_async<true>(lu, a.pivld[sys], g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x, blockDim.x);
+    else
+        solve_async<false>(lu, nullptr, g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x, blockDim.x);
 }
 
 // ------------------------------------------------------------------- S5
@@ -472,10 +478,6 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
         pf_set_error("fused step supports N <= 128");
         return PF_ERR_ARG;
     }
-    if (ctx->LDp.pivoted || ctx->LDm.pivoted || ctx->LDz.pivoted) {
-        pf_set_error("fused step: Helmholtz factors pivoted");
-        return PF_ERR_STATE;
-    }
     if (!corrector) {
         for (int i = 0; i < 3; ++i) std::swap(ctx->vel[i].d, ctx->prev[i].d);
         ctx->parity ^= 1;
@@ -494,7 +496,15 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
     a.rl[1] = ctx->s[6].d;
     a.rl[2] = ctx->s[3].d;  // free once the pressure is solved
     a.lnp = ctx->LNp.lu;
-    a.pivd = ctx->LNp_pivd;
+    a.pivd = ctx->LNp.pivd;
+    const pf_lumesh *ld[3] = {&ctx->LDp, &ctx->LDm, &ctx->LDz};
+    bool anyld = false;
+    for (int i = 0; i < 3; ++i) {
+        a.pivld[i] = ld[i]->pivd;
+        a.ldpiv[i] = ld[i]->pivoted;
+        anyld |= ld[i]->pivoted != 0;
+    }
+    const int ldsw = anyld ? KV + 1 : KL + 1;  // ring slot width of the Helmholtz solves
     a.ldp = ctx->LDp.lu;
     a.ldm = ctx->LDm.lu;
     a.ldz = ctx->LDz.lu;
@@ -513,7 +523,7 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
     static bool attrs_set = false;
     if (!attrs_set) {
         PF_CUDA(cudaFuncSetAttribute(k_solve_ld, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(192 * RING * (KL + 1) * sizeof(double))));
+                                     (int)(192 * RING * (KV + 1) * sizeof(double))));
         PF_CUDA(cudaFuncSetAttribute(k_solve_pnp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(64 * RING * (KV + 1) * sizeof(double))));
         attrs_set = true;
@@ -535,7 +545,7 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
     PF_LAUNCHED(ctx);
     {
         ProfScope ps_(ctx, PF_K_LUSOLVE);
-        k_solve_ld<<<tiles, 192, (size_t)192 * RING * (KL + 1) * sizeof(double), ctx->stream>>>(a);
+        k_solve_ld<<<tiles, 192, (size_t)192 * RING * ldsw * sizeof(double), ctx->stream>>>(a);
     }
     PF_LAUNCHED(ctx);
     if (corrector) PF_CUDA(cudaMemsetAsync(&ctx->dsc->dterr2_bits, 0, sizeof(unsigned long long), ctx->stream));

@@ -88,9 +88,7 @@ static int vel_step(pf_ctx *ctx) {
 
 bool pf_fused_step_ok(const pf_ctx *ctx);
 static bool fused_step_ok(const pf_ctx *ctx) { return pf_fused_step_ok(ctx); }
-bool pf_fused_step_ok(const pf_ctx *ctx) {
-    return ctx->g.N <= 128 && !ctx->LDp.pivoted && !ctx->LDm.pivoted && !ctx->LDz.pivoted;
-}
+bool pf_fused_step_ok(const pf_ctx *ctx) { return ctx->g.N <= 128; }
 
 // velocity.f90:400-410
 extern "C" int pf_vel_predictor(pf_ctx *ctx) {

@@ -127,6 +127,9 @@ _SIGS = {
     "pf_batch_matrices": [P],
     "pf_batch_step": [P, I, I, C.POINTER(C.c_longlong)],
     "pf_batch_sync": [P],
+    "pf_batch_stream": [P, PP],
+    "pf_batch_prof_enable": [P, I],
+    "pf_batch_prof_read": [P, I, DP, C.POINTER(C.c_ulonglong)],
     "pf_ctx_launches": [P, C.POINTER(C.c_ulonglong)],
     "pf_prof_enable": [P, I],
     "pf_prof_read": [P, I, DP, C.POINTER(C.c_ulonglong)],

@@ -525,6 +525,26 @@ class Batch:
     def sync(self):
         _check(self.lib.pf_batch_sync(self.h))
 
+    def prof_enable(self, on=True):
+        """on: True (all kernel categories), False, or a list of category names."""
+        cats = Pipe.KERNEL_CATEGORIES
+        if on is True:
+            mask = (1 << len(cats)) - 1
+        elif not on:
+            mask = 0
+        else:
+            mask = sum(1 << cats.index(n) for n in on)
+        _check(self.lib.pf_batch_prof_enable(self.h, mask))
+
+    def prof_read(self):
+        """{category: (total ms, launches)} summed over the pipes."""
+        out = {}
+        for i, name in enumerate(Pipe.KERNEL_CATEGORIES):
+            ms, n = C.c_double(), C.c_ulonglong()
+            _check(self.lib.pf_batch_prof_read(self.h, i, C.byref(ms), C.byref(n)))
+            out[name] = (ms.value, n.value)
+        return out
+
     def close(self):
         if self.h:
             for p in self.pipes:

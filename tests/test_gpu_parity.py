@@ -292,3 +292,25 @@ def test_multi_corrector_graph_path_parity():
     assert max(counts) >= 2
     assert O.rel_l2(state_from_dev(g), o.state()) <= 1e-12
     assert g.launches() > 0
+
+
+PIVOTING = dict(N=64, K=4, M=4, Mp=1, Re=1900.0, alpha=1.2, dt=0.01)  # Helmholtz factors pivot
+
+
+def test_pivoting_helmholtz_fused_path_parity():
+    """At N=64 and Re~1900 dgbtrf pivots in the u+-/uz systems too; the fused
+    step then uses the pivoting sweep for them."""
+    o, g = oracle_pipe(PIVOTING), device_pipe(PIVOTING)
+    o.vel_matrices()
+    g.vel_matrices()
+    for lu in (o.LDp, o.LDm, o.LDz):
+        assert (lu[1] != np.arange(o.N)[None, :]).any()
+    st = O.seeded_state(o, 12, 1e-3)
+    o.set_state(*st)
+    state_to_dev(g, st)
+    for _ in range(5):
+        assert o.timestep() == g.timestep()
+    assert O.rel_l2(state_from_dev(g), o.state()) <= 1e-12
+    o.vel_predictor()
+    g.vel_predictor()
+    assert O.rel_l2(state_from_dev(g), o.state()) <= 1e-12
