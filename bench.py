@@ -354,14 +354,15 @@ def run_batched(args, torch, P, dist, world, rank, local):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    n0 = sum(p.launches() for p in batch.pipes)
+    n0 = batch.launches()
+    staged = batch.staged()
     ev0, ev1 = dev_timer(torch, master)
     with ClockSampler(local) as clk:
         ev0.record(master)
         passes = batch.step(args.steps)
         ev1.record(master)
         master.synchronize()
-    launches = sum(p.launches() for p in batch.pipes) - n0
+    launches = batch.launches() - n0
     ms = ev0.elapsed_time(ev1)
     dom_ms, dom_n = batch.prof_read()[dom]
     batch.prof_enable(False)
@@ -389,10 +390,12 @@ def run_batched(args, torch, P, dist, world, rank, local):
     S = [coll_bytes(d) for d in cfgs]
     nc = passes / (args.steps * args.pipes)
     step_bytes = sum(s * (15 + 21 * nc) for s in S)
-    # dominant category: algorithmic bytes per launch averaged over the pipes
-    per_launch = PER_LAUNCH_S[dom] * sum(S) / len(S)
+    # dominant category: algorithmic bytes per launch; a stage-batched launch
+    # covers every pipe, a per-pipe launch one pipe (averaged over the pipes)
+    per_launch = PER_LAUNCH_S[dom] * (sum(S) if staged else sum(S) / len(S))
     io = sum(6 * d["N"] * harmonics_count(d) * 8 for d in cfgs)
     extra = {"corrector_iterations_per_step": nc, "algorithmic_bytes_per_batch_step": step_bytes,
+             "stage_batched": staged,
              "batch_step_ms": ms / args.steps,
              "step_roofline": {"bound": "hbm", "scope": "whole batch step (all stages, all pipes)",
                                "achieved": step_bytes / (ms / args.steps / 1e3) / 1e9, "unit": "GB/s"}}

@@ -225,11 +225,13 @@ int pf_diag_friction(pf_ctx *ctx, double *Ub, double *Uc, double *Ufr);
 
 /* ----------------------------------------------------------------- batches */
 /* Many independent pipes of uneven (N, K, M, Re, alpha, dt) advanced together;
- * one timestep of the batch is a single CUDA graph with one kernel chain per
- * pipe.  Each pipe's arithmetic is the lone-pipe path, so results are the
- * same alone and in the batch.  No single reference routine: this drives
- * the main.f90 loop body (main.f90:20-44) or steporbit's (newton.f90:740-762)
- * for every pipe. */
+ * one timestep of the batch is a single CUDA graph.  Where every pipe fits
+ * the batched kernels (fixed dt, N <= 128, transform lengths <= 192, one
+ * precision, mean-mode symmetry only) each stage is one launch over the tiles
+ * of all pipes; otherwise the graph holds one kernel chain per pipe.  Each
+ * pipe's arithmetic is the lone-pipe path, so results are the same alone and
+ * in the batch.  No single reference routine: this drives the main.f90 loop
+ * body (main.f90:20-44) or steporbit's (newton.f90:740-762) for every pipe. */
 typedef struct pf_batch pf_batch;
 int pf_batch_create(int npipes, const pf_config *cfgs, int device, pf_batch **out);
 int pf_batch_destroy(pf_batch *b);
@@ -249,6 +251,10 @@ int pf_batch_stream(pf_batch *b, void **stream);
  * time, so per-launch durations here include the sharing of the GPU. */
 int pf_batch_prof_enable(pf_batch *b, int mask);
 int pf_batch_prof_read(pf_batch *b, int cat, double *ms, unsigned long long *launches);
+/* Kernels launched so far by the batch (its pipes' and its batched ones). */
+int pf_batch_launches(pf_batch *b, unsigned long long *n);
+/* *staged = 1 when the batch's graphs launch each stage once for all pipes. */
+int pf_batch_staged(pf_batch *b, int *staged);
 
 /* ------------------------------------------------------- instrumentation */
 /* Kernel categories timed by CUDA events when profiling is on (the reference

@@ -1,21 +1,48 @@
 // Many independent pipes of uneven size advanced together.
 //
 // Each pipe is a full pf_ctx (its own fields, factors and stream).  One
-// timestep of the whole batch is a single CUDA graph: a fork event on the
-// batch's master stream, then on every pipe's stream that pipe's imposesym,
-// nonlinear terms, predictor, nonlinear terms and corrector (the same
-// kernels as a lone pipe, so every pipe's result is bit-identical alone and
-// in the batch), a copy of the pipe's device scalars to pinned host memory,
-// and a join back into the master stream.  The pipes' kernel chains are
-// independent graph branches, so the GPU runs them concurrently.
+// timestep of the whole batch is a single CUDA graph, built one of two ways:
 //
-// After the replay one host synchronisation reads every pipe's corrector
-// error; the reference's corrector control (timestep.f90:214-253) is then
-// applied per pipe, and the rare pipe that needs another corrector pass gets
-// it on its own stream (main.f90:35-41).  In orbit mode every pipe takes
+//  * stage-batched (the usual case: fixed dt, N <= 128, transform lengths up
+//    to 192, one precision, no symmetry beyond the mean-mode one): every stage
+//    of the step is ONE launch over the tiles of all pipes (a (pipe, tile) map
+//    per stage), so a step of the whole batch is about twenty kernels that
+//    each fill the GPU, whatever the mix of sizes;
+//  * branch graph (otherwise): on every pipe's stream that pipe's own chain of
+//    kernels, as a lone pipe runs it; the chains are independent graph
+//    branches and run concurrently.
+//
+// Both run the same per-tile code as a lone pipe, so every pipe's result is
+// bit-identical alone and in the batch.  After the replay one host
+// synchronisation reads every pipe's corrector error (gathered into one
+// pinned copy); the reference's corrector control (timestep.f90:214-253) is
+// then applied per pipe, and the rare pipe that needs another corrector pass
+// gets it on its own stream (main.f90:35-41).  In orbit mode every pipe takes
 // exactly one corrector pass (newton.f90:740-762).
 #include <cmath>
 #include "pf_internal.cuh"
+
+struct SymArgs {  // one pipe's velocity in one pointer state
+    double2 *u[3];
+    int N, Hp;
+};
+
+// variables.f90:611-616 (the mean-mode symmetry) for every pipe: block = pipe
+__global__ void k_batch_sym0(const SymArgs *__restrict__ s) {
+    const SymArgs &a = s[blockIdx.x];
+    for (int n = threadIdx.x; n < a.N; n += blockDim.x) {
+        const size_t at = (size_t)n * a.Hp;
+        a.u[0][at] = make_double2(0.0, 0.0);
+        a.u[1][at].y = 0.0;
+        a.u[2][at].y = 0.0;
+    }
+}
+
+// every pipe's device scalars into one array, read back with one copy
+__global__ void k_batch_scalars(DevScalars *const *__restrict__ src, DevScalars *__restrict__ dst, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = *src[i];
+}
 
 struct pf_batch {
     int n;
@@ -36,7 +63,40 @@ struct pf_batch {
     };
     std::vector<Ev> gev[2][2];
     std::vector<unsigned long long> gnp[2][2];  // kernels per pipe in each graph
+    // stage-batched launches
+    bool staged;                     // the graphs are stage-batched
+    pf_nl_batch *nlb;
+    pf_step_batch *stb;
+    int par0;                        // the pipes' pointer parity when nlb/stb were built
+    unsigned long long gen0;         // sum of the pipes' matrices generations then
+    SymArgs *d_sym[2];               // [pointer state]
+    DevScalars **d_scp;              // each pipe's device scalars
+    DevScalars *d_scall;             // gathered scalars
+    pf_stage_prof sprof;             // stage timing of the batched launches
+    std::vector<pf_stage_prof::Open> sev[2][2];
+    unsigned long long launches;     // batched kernels launched (not per pipe)
 };
+
+static void staged_free(pf_batch *b) {
+    pf_nl_batch_free(b->nlb);
+    pf_step_batch_free(b->stb);
+    b->nlb = nullptr;
+    b->stb = nullptr;
+    for (int s = 0; s < 2; ++s) {
+        cudaFree(b->d_sym[s]);
+        b->d_sym[s] = nullptr;
+    }
+    cudaFree(b->d_scp);
+    cudaFree(b->d_scall);
+    b->d_scp = nullptr;
+    b->d_scall = nullptr;
+}
+
+static unsigned long long matrices_gen(const pf_batch *b) {
+    unsigned long long s = 0;
+    for (const pf_ctx *c : b->pipes) s += c->matrices_gen;
+    return s;
+}
 
 // Destroy the batch graphs and hand their event pairs back to the pipes.
 static void batch_graphs_reset(pf_batch *b) {
@@ -50,7 +110,14 @@ static void batch_graphs_reset(pf_batch *b) {
                 b->pipes[e.pipe]->ev_pool.push_back(e.b);
             }
             b->gev[o][p].clear();
+            for (auto &e : b->sev[o][p]) {
+                b->sprof.pool.push_back(e.a);
+                b->sprof.pool.push_back(e.b);
+            }
+            b->sev[o][p].clear();
         }
+    staged_free(b);
+    b->staged = false;
 }
 
 static void batch_free(pf_batch *b) {
@@ -59,6 +126,11 @@ static void batch_free(pf_batch *b) {
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->master) cudaStreamDestroy(b->master);
     if (b->hsc) cudaFreeHost(b->hsc);
+    for (auto &e : b->sprof.open) {
+        b->sprof.pool.push_back(e.a);
+        b->sprof.pool.push_back(e.b);
+    }
+    for (cudaEvent_t e : b->sprof.pool) cudaEventDestroy(e);
     for (pf_ctx *c : b->pipes) pf_ctx_destroy(c);
     delete b;
 }
@@ -119,6 +191,98 @@ static bool batch_graphable(const pf_batch *b) {
         if (!(c->cfg.dt > 0.0 && c->matrices_ready && pf_nl_fused_supported(c) && pf_fused_step_ok(c)))
             return false;
     return true;
+}
+
+// Whether the stage-batched kernels cover every pipe of the batch.
+static bool batch_stageable(const pf_batch *b) {
+    for (const pf_ctx *c : b->pipes)
+        if (c->cfg.mirrorsym || c->cfg.shiftrefl || c->cfg.shiftrott || c->parity != b->pipes[0]->parity)
+            return false;
+    return pf_nl_batch_supported(b->pipes.data(), b->n);
+}
+
+// Per-pipe arguments of the stage-batched kernels for both pointer states.
+static int staged_build(pf_batch *b) {
+    staged_free(b);
+    PF_TRY(pf_nl_batch_build(b->pipes.data(), b->n, &b->nlb));
+    PF_TRY(pf_step_batch_build(b->pipes.data(), b->n, &b->stb));
+    std::vector<SymArgs> sym(b->n);
+    std::vector<DevScalars *> scp(b->n);
+    for (int s = 0; s < 2; ++s) {
+        for (int i = 0; i < b->n; ++i) {
+            const pf_ctx *c = b->pipes[i];
+            for (int k = 0; k < 3; ++k) sym[i].u[k] = s ? c->prev[k].d : c->vel[k].d;
+            sym[i].N = c->g.N;
+            sym[i].Hp = c->g.Hp;
+        }
+        PF_CUDA(cudaMalloc((void **)&b->d_sym[s], b->n * sizeof(SymArgs)));
+        PF_CUDA(cudaMemcpy(b->d_sym[s], sym.data(), b->n * sizeof(SymArgs), cudaMemcpyHostToDevice));
+    }
+    for (int i = 0; i < b->n; ++i) scp[i] = b->pipes[i]->dsc;
+    PF_CUDA(cudaMalloc((void **)&b->d_scp, b->n * sizeof(DevScalars *)));
+    PF_CUDA(cudaMemcpy(b->d_scp, scp.data(), b->n * sizeof(DevScalars *), cudaMemcpyHostToDevice));
+    PF_CUDA(cudaMalloc((void **)&b->d_scall, b->n * sizeof(DevScalars)));
+    b->par0 = b->pipes[0]->parity;
+    b->gen0 = matrices_gen(b);
+    return PF_OK;
+}
+
+// The stage-batched step: imposesym, nonlinear terms, predictor, nonlinear
+// terms, corrector (and imposesym in orbit mode) of every pipe, then the
+// gathered device scalars to pinned host memory.
+static int staged_body(pf_batch *b, int orbit, int par, unsigned long long *nk) {
+    const int s0 = par ^ b->par0, s1 = s0 ^ 1;  // pointer state before / after the predictor's swap
+    cudaStream_t st = b->master;
+    pf_stage_prof *pr = &b->sprof;
+    {
+        StageScope ss_(pr, PF_K_EW, st);
+        k_batch_sym0<<<b->n, 64, 0, st>>>(b->d_sym[s0]);
+    }
+    PF_CHECK_LAUNCH();
+    ++*nk;
+    PF_TRY(pf_nl_batch_launch(b->nlb, s0, st, pr, nk));
+    PF_TRY(pf_step_batch_launch(b->stb, s1, 0, st, pr, nk));
+    PF_TRY(pf_nl_batch_launch(b->nlb, s1, st, pr, nk));
+    PF_TRY(pf_step_batch_launch(b->stb, s1, 1, st, pr, nk));
+    if (orbit) {
+        {
+            StageScope ss_(pr, PF_K_EW, st);
+            k_batch_sym0<<<b->n, 64, 0, st>>>(b->d_sym[s1]);
+        }
+        PF_CHECK_LAUNCH();
+        ++*nk;
+    }
+    {
+        StageScope ss_(pr, PF_K_EW, st);
+        k_batch_scalars<<<grid1(b->n, 128), 128, 0, st>>>(b->d_scp, b->d_scall, b->n);
+    }
+    PF_CHECK_LAUNCH();
+    ++*nk;
+    PF_CUDA(cudaMemcpyAsync(b->hsc, b->d_scall, b->n * sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+    return PF_OK;
+}
+
+static int staged_capture(pf_batch *b, int orbit, int par, cudaGraphExec_t *exec, unsigned long long *nk) {
+    const size_t open0 = b->sprof.open.size();
+    cudaGraph_t graph = nullptr;
+    *nk = 0;
+    PF_CUDA(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
+    const int s = staged_body(b, orbit, par, nk);
+    const cudaError_t e = cudaStreamEndCapture(b->master, &graph);
+    for (size_t k = open0; k < b->sprof.open.size(); ++k) b->sev[orbit][par].push_back(b->sprof.open[k]);
+    b->sprof.open.resize(open0);
+    if (s != PF_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (s == PF_OK) pf_set_error("batch graph capture failed: %s", cudaGetErrorString(e));
+        return s == PF_OK ? PF_ERR_CUDA : s;
+    }
+    const cudaError_t e2 = cudaGraphInstantiate(exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) {
+        pf_set_error("batch graph instantiation failed: %s", cudaGetErrorString(e2));
+        return PF_ERR_CUDA;
+    }
+    return PF_OK;
 }
 
 // one pipe's body of the batch graph
@@ -219,15 +383,37 @@ extern "C" int pf_batch_step(pf_batch *b, int nsteps, int orbit, long long *corr
                 pf_set_error("pf_batch_step: pipes out of step (pointer parity differs)");
                 return PF_ERR_STATE;
             }
-        if (!b->g[orbit][p]) PF_TRY(batch_capture(b, orbit, p, &b->g[orbit][p], &b->gn[orbit][p]));
+        // the graphs bake in each pipe's factor sets and 1/dt
+        if (matrices_gen(b) != b->gen0) batch_graphs_reset(b);
+        if (!b->g[orbit][p]) {
+            if (!(b->g[0][0] || b->g[0][1] || b->g[1][0] || b->g[1][1])) {  // choose the graph kind
+                b->gen0 = matrices_gen(b);
+                b->staged = batch_stageable(b);
+                if (b->staged) PF_TRY(staged_build(b));
+            }
+            if (b->staged) PF_TRY(staged_capture(b, orbit, p, &b->g[orbit][p], &b->gn[orbit][p]));
+            else PF_TRY(batch_capture(b, orbit, p, &b->g[orbit][p], &b->gn[orbit][p]));
+        }
         PF_CUDA(cudaGraphLaunch(b->g[orbit][p], b->master));
         for (pf_ctx *c : b->pipes) {
             for (int i = 0; i < 3; ++i) std::swap(c->vel[i].d, c->prev[i].d);
             c->parity ^= 1;
             c->cfl_fused = true;
         }
-        for (int i = 0; i < b->n; ++i) b->pipes[i]->launches += b->gnp[orbit][p][i];
+        if (b->staged)
+            b->launches += b->gn[orbit][p];
+        else
+            for (int i = 0; i < b->n; ++i) b->pipes[i]->launches += b->gnp[orbit][p][i];
         PF_CUDA(cudaStreamSynchronize(b->master));
+        for (auto &e : b->sev[orbit][p]) {  // stage times of the batched launches
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
+                b->sprof.ms[e.cat] += ms;
+                b->sprof.n[e.cat] += 1;
+            } else {
+                cudaGetLastError();
+            }
+        }
         for (auto &e : b->gev[orbit][p]) {  // kernel times of the profiled categories
             float ms = 0.f;
             pf_ctx *c = b->pipes[e.pipe];
@@ -275,10 +461,15 @@ extern "C" int pf_batch_sync(pf_batch *b) {
 // the batch, inside the batch graphs; each call clears the totals.
 extern "C" int pf_batch_prof_enable(pf_batch *b, int mask) {
     PF_ARG(b, "null batch");
-    bool changed = false;
+    bool changed = b->sprof.mask != mask;
     for (pf_ctx *c : b->pipes) changed |= (c->prof_mask != mask);
     if (changed) batch_graphs_reset(b);
     for (pf_ctx *c : b->pipes) PF_TRY(pf_prof_enable(c, mask));
+    b->sprof.mask = mask;
+    for (int c = 0; c < PF_K_NCAT; ++c) {
+        b->sprof.ms[c] = 0.0;
+        b->sprof.n[c] = 0;
+    }
     return PF_OK;
 }
 
@@ -294,8 +485,25 @@ extern "C" int pf_batch_prof_read(pf_batch *b, int cat, double *ms, unsigned lon
         t += m;
         n += k;
     }
-    if (ms) *ms = t;
-    if (launches) *launches = n;
+    if (ms) *ms = t + b->sprof.ms[cat];
+    if (launches) *launches = n + b->sprof.n[cat];
+    return PF_OK;
+}
+
+// Kernels launched by the batch: the pipes' own plus the batched ones.
+extern "C" int pf_batch_launches(pf_batch *b, unsigned long long *n) {
+    PF_ARG(b && n, "pf_batch_launches: bad argument");
+    unsigned long long t = b->launches;
+    for (const pf_ctx *c : b->pipes) t += c->launches;
+    *n = t;
+    return PF_OK;
+}
+
+// 1 when the batch's graphs are stage-batched (one launch per stage over
+// every pipe), 0 for per-pipe graph branches or before the first graph.
+extern "C" int pf_batch_staged(pf_batch *b, int *staged) {
+    PF_ARG(b && staged, "pf_batch_staged: bad argument");
+    *staged = b->staged ? 1 : 0;
     return PF_OK;
 }
 

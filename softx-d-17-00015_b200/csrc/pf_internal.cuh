@@ -156,6 +156,7 @@ struct pf_ctx {
     pf_lumesh LNp, LDp, LDm, LDz;
     pf_mesh Ltp, Ltm, Ltz;
     bool LNp_set, matrices_ready;
+    unsigned long long matrices_gen;  // bumped by every vel_matrices
     double vel_nu;
     double *U;           // influence solutions [(c*N + n)*Hp + nh], c=0..5
     double *Ainv;        // inverted 4x4 [(i*4+j)*Hp + nh] == A(i+1,j+1,nh)
@@ -234,6 +235,12 @@ inline double bits_to_double(unsigned long long b) {
     std::memcpy(&d, &b, sizeof(d));
     return d;
 }
+// p[i] for i in 0..2 without indexing the array at run time, so a struct
+// of pointers copied into a kernel stays in registers
+template <typename T> __device__ __forceinline__ T pick3(T const (&p)[3], int i) {
+    return i == 0 ? p[0] : (i == 1 ? p[1] : p[2]);
+}
+
 inline unsigned grid1(long long n, int block) {
     return (unsigned)((n + block - 1) / block);
 }
@@ -272,6 +279,60 @@ int pf_launch_phys2coll(pf_ctx *ctx, int ncomp, const double *const *src,
 int pf_launch_maxtstep(pf_ctx *ctx, double *dt3);
 int pf_norm_host(pf_ctx *ctx, const double2 *a, double *E, double *Ek, double *Em);
 bool pf_nl_fused_supported(const pf_ctx *ctx);
+
+// Batched launches: one launch per stage over the tiles of many pipes.
+// Stage timing of such launches (event pairs on the launching stream, made
+// external while it is captured) is kept per category in a pf_stage_prof.
+struct pf_stage_prof {
+    int mask = 0;
+    std::vector<cudaEvent_t> pool;  // free events
+    struct Open {
+        int cat;
+        cudaEvent_t a, b;
+    };
+    std::vector<Open> open;  // recorded pairs not yet read
+    double ms[PF_K_NCAT] = {};
+    unsigned long long n[PF_K_NCAT] = {};
+    cudaEvent_t get() {
+        cudaEvent_t e = nullptr;
+        if (!pool.empty()) {
+            e = pool.back();
+            pool.pop_back();
+        } else {
+            cudaEventCreate(&e);
+        }
+        return e;
+    }
+};
+struct StageScope {
+    pf_stage_prof *p;
+    int cat;
+    cudaStream_t s;
+    cudaEvent_t a;
+    StageScope(pf_stage_prof *p_, int k, cudaStream_t s_) : p(p_), cat(k), s(s_), a(nullptr) {
+        if (p && (p->mask & (1 << k))) {
+            a = p->get();
+            pf_event_record(a, s);
+        }
+    }
+    ~StageScope() {
+        if (a) {
+            cudaEvent_t b = p->get();
+            pf_event_record(b, s);
+            p->open.push_back({cat, a, b});
+        }
+    }
+};
+struct pf_nl_batch;
+bool pf_nl_batch_supported(pf_ctx *const *pipes, int n);
+int pf_nl_batch_build(pf_ctx *const *pipes, int n, pf_nl_batch **out);
+int pf_nl_batch_launch(pf_nl_batch *b, int state, cudaStream_t st, pf_stage_prof *prof, unsigned long long *nk);
+void pf_nl_batch_free(pf_nl_batch *b);
+struct pf_step_batch;
+int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out);
+int pf_step_batch_launch(pf_step_batch *b, int state, int corrector, cudaStream_t st, pf_stage_prof *prof,
+                         unsigned long long *nk);
+void pf_step_batch_free(pf_step_batch *b);
 int pf_launch_nl_fused(pf_ctx *ctx);
 int pf_vel_step_fused(pf_ctx *ctx, int corrector);
 void pf_graphs_reset(pf_ctx *ctx);

@@ -454,6 +454,7 @@ int pf_vel_matrices_impl(pf_ctx *ctx) {
         return PF_ERR_SINGULAR;
     }
     ctx->matrices_ready = true;
+    ctx->matrices_gen++;
     return PF_OK;
 }
 

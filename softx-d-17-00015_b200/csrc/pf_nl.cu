@@ -14,6 +14,7 @@
 // The (m, z) intermediate T[((c*N + n)*M + m)*Z + z] is the only scratch;
 // the compute type C is double2 (FP64) or float2 (mixed precision).
 #include <cmath>
+#include <functional>
 #include "pf_internal.cuh"
 #include "pf_fftcore.cuh"
 
@@ -27,6 +28,9 @@ struct NLArgs {
     int const_flux;
     DevScalars *sc;
     unsigned long long *cfl;  // 3*N maxima as ordered bits
+    void *T;                  // (m, z) intermediate, compute type
+    const void *twz, *twt;    // twiddle tables, compute type
+    int MC, ZC;               // z-pass columns and theta-pass rows per block
 };
 
 template <typename C> __device__ __forceinline__ C to_c(double2 v);
@@ -50,7 +54,7 @@ __device__ __forceinline__ double2 band_row_d(const double *__restrict__ band, i
 __device__ __forceinline__ double2 nl_input(const NLArgs &a, int comp, int n, int nh, int k, int m) {
     const Geo &g = a.g;
     const size_t at = (size_t)n * g.Hp + nh;
-    if (comp < 3) return a.u[comp][at];
+    if (comp < 3) return pick3(a.u, comp)[at];
     const double rm1 = a.dm.rp[2 * g.N + n];
     const double m1r1 = rm1 * g.Mp * m;
     const double k1a1 = g.alpha * k;
@@ -69,15 +73,20 @@ __device__ __forceinline__ double2 nl_input(const NLArgs &a, int comp, int n, in
 }
 
 template <int ZL, typename C>
-__global__ void __launch_bounds__(NL_THREADS) k_nl_zinv(NLArgs a, C *__restrict__ T, const C *__restrict__ twz, int MC) {
+__device__ __forceinline__ void nl_zinv_body(const NLArgs &a, int bx, int by, int bz) {
     extern __shared__ __align__(16) unsigned char smraw[];
+    C *__restrict__ T = reinterpret_cast<C *>(a.T);
+    const C *__restrict__ twz = reinterpret_cast<const C *>(a.twz);
+    const int MC = a.MC;
+    if (a.cfl && bx == 0 && by == 0 && bz == 0)  // reset the CFL maxima the theta pass raises
+        for (int i = threadIdx.x; i < 3 * a.g.N; i += blockDim.x) a.cfl[i] = 0ull;
     using FR = FFTRows<ZL, C>;
     constexpr int RS = FR::pitch;
     C *rows = reinterpret_cast<C *>(smraw);
     C *tw = rows + (FR::smem_elems(MC) - 2 * ZL), *tw2 = tw + ZL;
     const Geo &g = a.g;
     const int K = g.K;
-    const int comp = blockIdx.z, n = blockIdx.y, m0 = blockIdx.x * MC;
+    const int comp = bz, n = by, m0 = bx * MC;
     const int mc = min(MC, g.M - m0);
     fft4_tables<ZL>(tw, tw2, twz);
     for (int idx = threadIdx.x; idx < mc * ZL; idx += blockDim.x) {
@@ -110,10 +119,13 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *p, double v) 
 }
 
 template <int TL, typename C>
-__global__ void __launch_bounds__(NL_THREADS) k_nl_theta(NLArgs a, C *__restrict__ T, const C *__restrict__ twt,
-                                                         int ZC, typename CTraits<C>::R scale) {
+__device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
     using R = typename CTraits<C>::R;
     extern __shared__ __align__(16) unsigned char smraw[];
+    C *__restrict__ T = reinterpret_cast<C *>(a.T);
+    const C *__restrict__ twt = reinterpret_cast<const C *>(a.twt);
+    const int ZC = a.ZC;
+    const R scale = (R)(1.0 / (double)(a.g.Z * a.g.Th));  // transform.fftw3.f90:114
     using FR = FFTRows<TL, C>;
     constexpr int RS = FR::pitch;
     const Geo &g = a.g;
@@ -122,7 +134,7 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_theta(NLArgs a, C *__restrict
     C *bufA = reinterpret_cast<C *>(smraw);
     C *bufB = bufA + (FR::smem_elems(rowsA) - 2 * TL);
     C *tw = bufB + (FR::smem_elems(rowsA / 2) - 2 * TL), *tw2 = tw + TL;
-    const int n = blockIdx.y, z0 = blockIdx.x * ZC;
+    const int n = by, z0 = bx * ZC;
     fft4_tables<TL>(tw, tw2, twt);
     for (int i = threadIdx.x; i < rowsA * RS; i += blockDim.x) bufA[i] = CTraits<C>::make(0, 0);
     __syncthreads();
@@ -200,16 +212,18 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_theta(NLArgs a, C *__restrict
 }
 
 template <int ZL, typename C>
-__global__ void __launch_bounds__(NL_THREADS) k_nl_zfwd(NLArgs a, const C *__restrict__ T, const C *__restrict__ twz,
-                                                        int MC) {
+__device__ __forceinline__ void nl_zfwd_body(const NLArgs &a, int bx, int by, int bz) {
     extern __shared__ __align__(16) unsigned char smraw[];
+    const C *__restrict__ T = reinterpret_cast<const C *>(a.T);
+    const C *__restrict__ twz = reinterpret_cast<const C *>(a.twz);
+    const int MC = a.MC;
     using FR = FFTRows<ZL, C>;
     constexpr int RS = FR::pitch;
     C *rows = reinterpret_cast<C *>(smraw);
     C *tw = rows + (FR::smem_elems(MC) - 2 * ZL), *tw2 = tw + ZL;
     const Geo &g = a.g;
     const int K = g.K;
-    const int comp = blockIdx.z, n = blockIdx.y, m0 = blockIdx.x * MC;
+    const int comp = bz, n = by, m0 = bx * MC;
     const int mc = min(MC, g.M - m0);
     fft4_tables<ZL>(tw, tw2, twz);
     const C *in = T + ((size_t)(comp * g.N + n) * g.M + m0) * ZL;
@@ -227,7 +241,7 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_zfwd(NLArgs a, const C *__res
         Pr0 = Pr0 / (-2.0);
         if (n == 0 && m0 == 0 && threadIdx.x == 0) a.sc->Pr0 = Pr0;
     }
-    double2 *f = a.N[comp] + (size_t)n * g.Hp;
+    double2 *f = pick3(a.N, comp) + (size_t)n * g.Hp;
     for (int idx = threadIdx.x; idx < mc * (2 * K - 1); idx += blockDim.x) {
         const int c = idx / (2 * K - 1), kk = idx - c * (2 * K - 1) - (K - 1);
         const int m = m0 + c;
@@ -243,12 +257,25 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_zfwd(NLArgs a, const C *__res
             o.y = o.y - av * vz.x + b * vr.y;
             if (nh == 0 && a.const_flux) o.x = o.x + 4.0 * Pr0 / g.Re;
         } else {
-            const double2 v = a.u[comp][at];
+            const double2 v = pick3(a.u, comp)[at];
             o.x = o.x + av * v.y;
             o.y = o.y - av * v.x;
         }
         f[nh] = o;
     }
+}
+
+template <int ZL, typename C>
+__global__ void __launch_bounds__(NL_THREADS) k_nl_zinv(NLArgs a) {
+    nl_zinv_body<ZL, C>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <int TL, typename C>
+__global__ void __launch_bounds__(NL_THREADS) k_nl_theta(NLArgs a) {
+    nl_theta_body<TL, C>(a, blockIdx.x, blockIdx.y);
+}
+template <int ZL, typename C>
+__global__ void __launch_bounds__(NL_THREADS) k_nl_zfwd(NLArgs a) {
+    nl_zfwd_body<ZL, C>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------------------ dispatch
@@ -280,29 +307,72 @@ template <typename C> static int rows_elems(int L, int B) {
     }
 }
 
-template <typename C>
-static int launch_nl(pf_ctx *ctx, const NLArgs &a, const C *twz, const C *twt) {
-    const Geo &g = ctx->g;
-    C *T = reinterpret_cast<C *>(ctx->T);
+// tiles and shared memory of one pipe's three launches
+template <typename C> struct NLTiles {
+    int MC, ZC;
+    size_t zsm, tsm;
+};
+template <typename C> static NLTiles<C> nl_tiles(const Geo &g) {
     const size_t cs = sizeof(C);
-    int MC = g.M;
-    while (MC > 1 && (size_t)rows_elems<C>(g.Z, MC) * cs > 64 * 1024) --MC;
-    const size_t zsm = (size_t)rows_elems<C>(g.Z, MC) * cs;
-    int ZC = 8;
-    while (ZC > 2 && (size_t)(rows_elems<C>(g.Th, 3 * ZC) + rows_elems<C>(g.Th, 3 * ZC / 2)) * cs > 64 * 1024) ZC -= 2;
-    const size_t tsm = (size_t)(rows_elems<C>(g.Th, 3 * ZC) + rows_elems<C>(g.Th, 3 * ZC / 2)) * cs;
-    const dim3 gz((g.M + MC - 1) / MC, g.N, 6), gt((g.Z + ZC - 1) / ZC, g.N), gf((g.M + MC - 1) / MC, g.N, 3);
-    const typename CTraits<C>::R scale = (typename CTraits<C>::R)(1.0 / (double)(g.Z * g.Th));
+    NLTiles<C> t;
+    t.MC = g.M;
+    while (t.MC > 1 && (size_t)rows_elems<C>(g.Z, t.MC) * cs > 64 * 1024) --t.MC;
+    t.zsm = (size_t)rows_elems<C>(g.Z, t.MC) * cs;
+    t.ZC = 8;
+    while (t.ZC > 2 && (size_t)(rows_elems<C>(g.Th, 3 * t.ZC) + rows_elems<C>(g.Th, 3 * t.ZC / 2)) * cs > 64 * 1024)
+        t.ZC -= 2;
+    t.tsm = (size_t)(rows_elems<C>(g.Th, 3 * t.ZC) + rows_elems<C>(g.Th, 3 * t.ZC / 2)) * cs;
+    return t;
+}
+
+// The fused-transform arguments of one pipe in its current pointer state.
+static NLArgs make_nl_args(pf_ctx *ctx) {
+    NLArgs a;
+    for (int i = 0; i < 3; ++i) {
+        a.u[i] = ctx->vel[i].d;
+        a.N[i] = ctx->vel[3 + i].d;
+    }
+    a.dm = ctx->dm;
+    a.g = ctx->g;
+    a.const_flux = ctx->cfg.const_flux;
+    a.sc = ctx->dsc;
+    a.cfl = ctx->cflmax;
+    a.T = ctx->T;
+    const bool mixed = ctx->cfg.precision == PF_PREC_MIXED;
+    a.twz = mixed ? (const void *)ctx->twZf : (const void *)ctx->twZ;
+    a.twt = mixed ? (const void *)ctx->twTf : (const void *)ctx->twT;
+    if (mixed) {
+        const NLTiles<float2> t = nl_tiles<float2>(ctx->g);
+        a.MC = t.MC;
+        a.ZC = t.ZC;
+    } else {
+        const NLTiles<double2> t = nl_tiles<double2>(ctx->g);
+        a.MC = t.MC;
+        a.ZC = t.ZC;
+    }
+    return a;
+}
+
+template <typename K> static int raise_smem(K kernel, size_t bytes, size_t &cur) {
+    if (bytes > cur) {
+        PF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        cur = bytes;
+    }
+    return PF_OK;
+}
+
+template <typename C>
+static int launch_nl(pf_ctx *ctx, const NLArgs &a) {
+    const Geo &g = ctx->g;
+    const NLTiles<C> t = nl_tiles<C>(g);
+    const dim3 gz((g.M + t.MC - 1) / t.MC, g.N, 6), gt((g.Z + t.ZC - 1) / t.ZC, g.N), gf((g.M + t.MC - 1) / t.MC, g.N, 3);
     switch (g.Z) {
-#define PF_CASE(L)                                                                                   \
-    case L: {                                                                                        \
-        static size_t set_ = 0;                                                                      \
-        if (zsm > set_) {                                                                              \
-            PF_CUDA(cudaFuncSetAttribute(k_nl_zinv<L, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsm)); \
-            set_ = zsm;                                                                               \
-        }                                                                                            \
-        ProfScope ps_(ctx, PF_K_ZINV);                                                               \
-        k_nl_zinv<L, C><<<gz, NL_THREADS, zsm, ctx->stream>>>(a, T, twz, MC);                        \
+#define PF_CASE(L)                                                    \
+    case L: {                                                         \
+        static size_t set_ = 0;                                       \
+        PF_TRY(raise_smem(k_nl_zinv<L, C>, t.zsm, set_));             \
+        ProfScope ps_(ctx, PF_K_ZINV);                                \
+        k_nl_zinv<L, C><<<gz, NL_THREADS, t.zsm, ctx->stream>>>(a);   \
     } break;
         PF_NL_LENGTHS(PF_CASE)
 #undef PF_CASE
@@ -311,17 +381,13 @@ static int launch_nl(pf_ctx *ctx, const NLArgs &a, const C *twz, const C *twt) {
         return PF_ERR_ARG;
     }
     PF_LAUNCHED(ctx);
-    if (a.cfl) PF_CUDA(cudaMemsetAsync(a.cfl, 0, 3 * g.N * sizeof(unsigned long long), ctx->stream));
     switch (g.Th) {
-#define PF_CASE(L)                                                                                    \
-    case L: {                                                                                         \
-        static size_t set_ = 0;                                                                      \
-        if (tsm > set_) {                                                                              \
-            PF_CUDA(cudaFuncSetAttribute(k_nl_theta<L, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm)); \
-            set_ = tsm;                                                                               \
-        }                                                                                            \
-        ProfScope ps_(ctx, PF_K_THFWD);                                                               \
-        k_nl_theta<L, C><<<gt, NL_THREADS, tsm, ctx->stream>>>(a, T, twt, ZC, scale);                 \
+#define PF_CASE(L)                                                    \
+    case L: {                                                         \
+        static size_t set_ = 0;                                       \
+        PF_TRY(raise_smem(k_nl_theta<L, C>, t.tsm, set_));            \
+        ProfScope ps_(ctx, PF_K_THFWD);                               \
+        k_nl_theta<L, C><<<gt, NL_THREADS, t.tsm, ctx->stream>>>(a);  \
     } break;
         PF_NL_LENGTHS(PF_CASE)
 #undef PF_CASE
@@ -331,15 +397,12 @@ static int launch_nl(pf_ctx *ctx, const NLArgs &a, const C *twz, const C *twt) {
     }
     PF_LAUNCHED(ctx);
     switch (g.Z) {
-#define PF_CASE(L)                                                                                   \
-    case L: {                                                                                        \
-        static size_t set_ = 0;                                                                      \
-        if (zsm > set_) {                                                                              \
-            PF_CUDA(cudaFuncSetAttribute(k_nl_zfwd<L, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsm)); \
-            set_ = zsm;                                                                               \
-        }                                                                                            \
-        ProfScope ps_(ctx, PF_K_ZFWD);                                                               \
-        k_nl_zfwd<L, C><<<gf, NL_THREADS, zsm, ctx->stream>>>(a, T, twz, MC);                        \
+#define PF_CASE(L)                                                    \
+    case L: {                                                         \
+        static size_t set_ = 0;                                       \
+        PF_TRY(raise_smem(k_nl_zfwd<L, C>, t.zsm, set_));             \
+        ProfScope ps_(ctx, PF_K_ZFWD);                                \
+        k_nl_zfwd<L, C><<<gf, NL_THREADS, t.zsm, ctx->stream>>>(a);   \
     } break;
         PF_NL_LENGTHS(PF_CASE)
 #undef PF_CASE
@@ -352,21 +415,12 @@ static int launch_nl(pf_ctx *ctx, const NLArgs &a, const C *twz, const C *twt) {
 
 __global__ void k_nl_mean64(NLArgs a);
 
-// vel_transform + vel_nonlinear in three launches; CFL maxima per radial
-// point are left in ctx->cflmax.
+// vel_transform + vel_nonlinear in three launches (four in mixed precision);
+// CFL maxima per radial point are left in ctx->cflmax.
 int pf_launch_nl_fused(pf_ctx *ctx) {
-    NLArgs a;
-    for (int i = 0; i < 3; ++i) {
-        a.u[i] = ctx->vel[i].d;
-        a.N[i] = ctx->vel[3 + i].d;
-    }
-    a.dm = ctx->dm;
-    a.g = ctx->g;
-    a.const_flux = ctx->cfg.const_flux;
-    a.sc = ctx->dsc;
-    a.cfl = ctx->cflmax;
+    const NLArgs a = make_nl_args(ctx);
     if (ctx->cfg.precision == PF_PREC_MIXED) {
-        PF_TRY(launch_nl<float2>(ctx, a, ctx->twZf, ctx->twTf));
+        PF_TRY(launch_nl<float2>(ctx, a));
         {
             ProfScope ps_(ctx, PF_K_ZFWD);
             k_nl_mean64<<<ctx->g.N, 256, 0, ctx->stream>>>(a);
@@ -374,8 +428,9 @@ int pf_launch_nl_fused(pf_ctx *ctx) {
         PF_LAUNCHED(ctx);
         return PF_OK;
     }
-    return launch_nl<double2>(ctx, a, ctx->twZ, ctx->twT);
+    return launch_nl<double2>(ctx, a);
 }
+
 
 // ------------------------------------------------- FP64 mean mode (mixed)
 // With FP32 transforms the k=m=0 coefficient of u x curl(u) is replaced by
@@ -384,9 +439,8 @@ int pf_launch_nl_fused(pf_ctx *ctx) {
 //   mean(f g) = Re f00 Re g00 + 2 sum_{k>=1} Re(f_k0 conj g_k0)
 //             + 2 sum_{m>=1, all k} Re(f_km conj g_km)
 // (the c2r transform ignores Im f00).  One block per radial point.
-__global__ void k_nl_mean64(NLArgs a) {
+__device__ __forceinline__ void nl_mean64_body(const NLArgs &a, int n) {
     const Geo &g = a.g;
-    const int n = blockIdx.x;
     double s[3] = {0.0, 0.0, 0.0};
     for (int nh = threadIdx.x; nh < g.H; nh += blockDim.x) {
         int k, m;
@@ -425,4 +479,240 @@ __global__ void k_nl_mean64(NLArgs a) {
         a.N[1][at] = make_double2(t[1], 0.0);
         a.N[2][at] = make_double2(zr, (-a.dm.velUp[n]) * ur.y);
     }
+}
+
+__global__ void k_nl_mean64(NLArgs a) { nl_mean64_body(a, blockIdx.x); }
+
+// ------------------------------------------------------------------ batched
+// One launch per (stage, transform length) covers the blocks of every pipe
+// of a batch with that length: blk[b] = (pipe, block index within that pipe's
+// own grid), and each block runs the lone-pipe body.  The launches of one
+// stage for different lengths are independent and run concurrently (forked
+// onto auxiliary streams, joined before the next stage).
+template <int ZL, typename C>
+__global__ void __launch_bounds__(NL_THREADS) k_nl_zinv_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
+    const int2 pb = blk[blockIdx.x];
+    const NLArgs a = args[pb.x];  // by value: stores through its pointers cannot alias it
+    const int gx = (a.g.M + a.MC - 1) / a.MC;
+    nl_zinv_body<ZL, C>(a, pb.y % gx, (pb.y / gx) % a.g.N, pb.y / (gx * a.g.N));
+}
+
+template <int TL, typename C>
+__global__ void __launch_bounds__(NL_THREADS) k_nl_theta_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
+    const int2 pb = blk[blockIdx.x];
+    const NLArgs a = args[pb.x];
+    const int gx = (a.g.Z + a.ZC - 1) / a.ZC;
+    nl_theta_body<TL, C>(a, pb.y % gx, pb.y / gx);
+}
+
+template <int ZL, typename C>
+__global__ void __launch_bounds__(NL_THREADS) k_nl_zfwd_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
+    const int2 pb = blk[blockIdx.x];
+    const NLArgs a = args[pb.x];
+    const int gx = (a.g.M + a.MC - 1) / a.MC;
+    nl_zfwd_body<ZL, C>(a, pb.y % gx, (pb.y / gx) % a.g.N, pb.y / (gx * a.g.N));
+}
+
+__global__ void k_nl_mean64_batch(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
+    const int2 pb = blk[blockIdx.x];
+    const NLArgs a = args[pb.x];
+    nl_mean64_body(a, pb.y);
+}
+
+namespace {
+struct NLGroup {
+    int L;
+    int2 *blk;
+    int nblk;
+    size_t smem;
+};
+constexpr int NLB_STAGES = 3;  // zinv, theta, zfwd
+constexpr int NLB_MAXG = 12;   // transform lengths built
+}  // namespace
+
+struct pf_nl_batch {
+    bool mixed;
+    int n;
+    NLArgs *d_args[2];  // [pointer state]: 0 = as built, 1 = vel/prev swapped
+    std::vector<NLGroup> groups[NLB_STAGES];
+    int2 *mean_blk;
+    int nmean;
+    cudaStream_t aux[NLB_MAXG];
+    cudaEvent_t fork[NLB_STAGES], join[NLB_STAGES][NLB_MAXG];
+};
+
+bool pf_nl_batch_supported(pf_ctx *const *pipes, int n) {
+    if (n <= 0) return false;
+    const int prec = pipes[0]->cfg.precision;
+    for (int i = 0; i < n; ++i)
+        if (pipes[i]->cfg.precision != prec || !pf_nl_fused_supported(pipes[i])) return false;
+    return true;
+}
+
+void pf_nl_batch_free(pf_nl_batch *b) {
+    if (!b) return;
+    for (int s = 0; s < 2; ++s) cudaFree(b->d_args[s]);
+    for (int st = 0; st < NLB_STAGES; ++st) {
+        for (NLGroup &gr : b->groups[st]) cudaFree(gr.blk);
+        if (b->fork[st]) cudaEventDestroy(b->fork[st]);
+        for (int k = 0; k < NLB_MAXG; ++k)
+            if (b->join[st][k]) cudaEventDestroy(b->join[st][k]);
+    }
+    cudaFree(b->mean_blk);
+    for (int k = 0; k < NLB_MAXG; ++k)
+        if (b->aux[k]) cudaStreamDestroy(b->aux[k]);
+    delete b;
+}
+
+template <typename T> static int upload(T **d, const std::vector<T> &h) {
+    PF_CUDA(cudaMalloc((void **)d, std::max<size_t>(1, h.size()) * sizeof(T)));
+    if (!h.empty()) PF_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return PF_OK;
+}
+
+// blocks of stage st for the pipes whose length (Z or Th) is L, largest
+// pipes first
+template <typename C> static int nlb_groups(pf_nl_batch *b, pf_ctx *const *pipes, int n) {
+    for (int st = 0; st < NLB_STAGES; ++st) {
+        std::vector<int> lengths;
+        for (int i = 0; i < n; ++i) {
+            const int L = st == 1 ? pipes[i]->g.Th : pipes[i]->g.Z;
+            if (std::find(lengths.begin(), lengths.end(), L) == lengths.end()) lengths.push_back(L);
+        }
+        std::sort(lengths.begin(), lengths.end(), std::greater<int>());
+        for (int L : lengths) {
+            std::vector<int2> map;
+            size_t smem = 0;
+            for (int i = 0; i < n; ++i) {
+                const Geo &g = pipes[i]->g;
+                if ((st == 1 ? g.Th : g.Z) != L) continue;
+                const NLTiles<C> t = nl_tiles<C>(g);
+                int nb = 0;
+                if (st == 0) nb = ((g.M + t.MC - 1) / t.MC) * g.N * 6;
+                if (st == 1) nb = ((g.Z + t.ZC - 1) / t.ZC) * g.N;
+                if (st == 2) nb = ((g.M + t.MC - 1) / t.MC) * g.N * 3;
+                for (int l = 0; l < nb; ++l) map.push_back(make_int2(i, l));
+                smem = std::max(smem, st == 1 ? t.tsm : t.zsm);
+            }
+            NLGroup gr{L, nullptr, (int)map.size(), smem};
+            b->groups[st].push_back(gr);
+            PF_TRY(upload(&b->groups[st].back().blk, map));
+        }
+    }
+    std::vector<int2> mean;
+    for (int i = 0; i < n; ++i)
+        for (int l = 0; l < pipes[i]->g.N; ++l) mean.push_back(make_int2(i, l));
+    b->nmean = (int)mean.size();
+    return upload(&b->mean_blk, mean);
+}
+
+// Arguments of every pipe in both pointer states, and the per-length maps.
+int pf_nl_batch_build(pf_ctx *const *pipes, int n, pf_nl_batch **out) {
+    *out = nullptr;
+    if (!pf_nl_batch_supported(pipes, n)) {
+        pf_set_error("batched transforms: mixed precisions or a transform length not built");
+        return PF_ERR_ARG;
+    }
+    pf_nl_batch *b = new pf_nl_batch();
+    b->n = n;
+    b->mixed = pipes[0]->cfg.precision == PF_PREC_MIXED;
+    int s = PF_OK;
+    std::vector<NLArgs> h(n);
+    for (int st = 0; st < 2 && s == PF_OK; ++st) {
+        for (int i = 0; i < n; ++i) {
+            if (st) for (int c = 0; c < 3; ++c) std::swap(pipes[i]->vel[c].d, pipes[i]->prev[c].d);
+            h[i] = make_nl_args(pipes[i]);
+            if (st) for (int c = 0; c < 3; ++c) std::swap(pipes[i]->vel[c].d, pipes[i]->prev[c].d);
+        }
+        s = upload(&b->d_args[st], h);
+    }
+    if (s == PF_OK) s = b->mixed ? nlb_groups<float2>(b, pipes, n) : nlb_groups<double2>(b, pipes, n);
+    for (int st = 0; st < NLB_STAGES && s == PF_OK; ++st) {
+        if (cudaEventCreateWithFlags(&b->fork[st], cudaEventDisableTiming) != cudaSuccess) s = PF_ERR_CUDA;
+        for (size_t k = 0; k < b->groups[st].size() && s == PF_OK; ++k)
+            if (cudaEventCreateWithFlags(&b->join[st][k], cudaEventDisableTiming) != cudaSuccess) s = PF_ERR_CUDA;
+    }
+    for (int k = 0; k < NLB_MAXG && s == PF_OK; ++k)
+        if (cudaStreamCreateWithFlags(&b->aux[k], cudaStreamNonBlocking) != cudaSuccess) s = PF_ERR_CUDA;
+    if (s != PF_OK) {
+        if (s == PF_ERR_CUDA) pf_set_error("batched transforms: allocation failed");
+        pf_nl_batch_free(b);
+        return s;
+    }
+    *out = b;
+    return PF_OK;
+}
+
+template <typename C> static int nlb_group_launch(int st, const NLGroup &gr, const NLArgs *args, cudaStream_t s) {
+    switch (gr.L) {
+#define PF_CASE(L)                                                                                 \
+    case L: {                                                                                      \
+        static size_t set_[NLB_STAGES] = {0, 0, 0};                                                \
+        if (st == 0) {                                                                             \
+            PF_TRY(raise_smem(k_nl_zinv_b<L, C>, gr.smem, set_[0]));                               \
+            k_nl_zinv_b<L, C><<<gr.nblk, NL_THREADS, gr.smem, s>>>(args, gr.blk);                  \
+        } else if (st == 1) {                                                                      \
+            PF_TRY(raise_smem(k_nl_theta_b<L, C>, gr.smem, set_[1]));                              \
+            k_nl_theta_b<L, C><<<gr.nblk, NL_THREADS, gr.smem, s>>>(args, gr.blk);                 \
+        } else {                                                                                   \
+            PF_TRY(raise_smem(k_nl_zfwd_b<L, C>, gr.smem, set_[2]));                               \
+            k_nl_zfwd_b<L, C><<<gr.nblk, NL_THREADS, gr.smem, s>>>(args, gr.blk);                  \
+        }                                                                                          \
+    } break;
+        PF_NL_LENGTHS(PF_CASE)
+#undef PF_CASE
+    default:
+        pf_set_error("batched transforms: length %d not built", gr.L);
+        return PF_ERR_ARG;
+    }
+    PF_CHECK_LAUNCH();
+    return PF_OK;
+}
+
+// one stage: the first length on st, the others forked onto auxiliary streams
+template <typename C>
+static int nlb_stage(pf_nl_batch *b, int stage, const NLArgs *args, cudaStream_t st, unsigned long long *nk) {
+    const std::vector<NLGroup> &gs = b->groups[stage];
+    if (gs.size() > 1) {
+        PF_CUDA(cudaEventRecord(b->fork[stage], st));
+        for (size_t k = 1; k < gs.size(); ++k) PF_CUDA(cudaStreamWaitEvent(b->aux[k], b->fork[stage], 0));
+    }
+    for (size_t k = 0; k < gs.size(); ++k) {
+        PF_TRY(nlb_group_launch<C>(stage, gs[k], args, k ? b->aux[k] : st));
+        ++*nk;
+    }
+    for (size_t k = 1; k < gs.size(); ++k) {
+        PF_CUDA(cudaEventRecord(b->join[stage][k], b->aux[k]));
+        PF_CUDA(cudaStreamWaitEvent(st, b->join[stage][k], 0));
+    }
+    return PF_OK;
+}
+
+template <typename C>
+static int nlb_launch(pf_nl_batch *b, int state, cudaStream_t st, pf_stage_prof *prof, unsigned long long *nk) {
+    const NLArgs *args = b->d_args[state];
+    const int cats[NLB_STAGES] = {PF_K_ZINV, PF_K_THFWD, PF_K_ZFWD};
+    for (int stage = 0; stage < NLB_STAGES; ++stage) {
+        StageScope ss_(prof, cats[stage], st);
+        PF_TRY(nlb_stage<C>(b, stage, args, st, nk));
+    }
+    return PF_OK;
+}
+
+// vel_transform + vel_nonlinear of every pipe: one launch per stage and
+// transform length (mixed precision adds the FP64 mean-mode launch), counted
+// into *nk.  state 0: the pointers the pipes held when the batch was built;
+// 1: vel/prev swapped.
+int pf_nl_batch_launch(pf_nl_batch *b, int state, cudaStream_t st, pf_stage_prof *prof, unsigned long long *nk) {
+    if (b->mixed) {
+        PF_TRY(nlb_launch<float2>(b, state, st, prof, nk));
+        {
+            StageScope ss_(prof, PF_K_ZFWD, st);
+            k_nl_mean64_batch<<<b->nmean, 256, 0, st>>>(b->d_args[state], b->mean_blk);
+        }
+        PF_CHECK_LAUNCH();
+        *nk += 1;
+        return PF_OK;
+    }
+    return nlb_launch<double2>(b, state, st, prof, nk);
 }

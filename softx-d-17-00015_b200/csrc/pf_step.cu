@@ -54,12 +54,15 @@ __device__ __forceinline__ double lap_diag(const DevMesh &dm, const Geo &g, int 
 }
 
 // ------------------------------------------------------------------- S1
-__global__ void __launch_bounds__(TM *TR) k_step_rhs(StepArgs a) {
+__device__ __forceinline__ void step_rhs_body(const StepArgs &a, int bx) {
     extern __shared__ double2 rsm[];  // [N][TM]: radial component of pm2rt(rhs)
     const Geo &g = a.g;
     const int N = g.N, Hp = g.Hp;
     const int tx = threadIdx.x % TM, ty = threadIdx.x / TM;
-    const int nh = blockIdx.x * TM + tx;
+    const int nh = bx * TM + tx;
+    // the corrector's error max (timestep.f90:190-207) restarts here; S5
+    // accumulates it after every block of this launch has finished
+    if (a.mode == 1 && bx == 0 && threadIdx.x == 0) a.sc->dterr2_bits = 0ull;
     const bool live = nh < g.H;
     int k = 0, m = 0;
     if (live) mode_km(nh, g.K, k, m);
@@ -271,11 +274,11 @@ __device__ __forceinline__ void solve_async(const double *__restrict__ lu, const
 }
 
 // S2: warp = (re or im) of 32 consecutive modes
-__global__ void __launch_bounds__(64) k_solve_pnp(StepArgs a) {
+__device__ __forceinline__ void solve_pnp_body(const StepArgs &a, int bx) {
     extern __shared__ double ring2[];
     const Geo &g = a.g;
     const int part = threadIdx.x >> 5;
-    const int nh = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int nh = bx * 32 + (threadIdx.x & 31);
     const bool live = nh < g.H;
     const size_t st = 2 * (size_t)g.Hp;
     double *out = reinterpret_cast<double *>(a.p) + 2 * (size_t)nh + part;
@@ -290,9 +293,9 @@ __global__ void __launch_bounds__(64) k_solve_pnp(StepArgs a) {
 
 // S3: rhs - rt2pm(grad p) (velocity.f90:232-236) with zero boundary rows
 // (velocity.f90:376-378), one thread per (n, mode)
-__global__ void k_step_proj(StepArgs a) {
+__device__ __forceinline__ void step_proj_body(const StepArgs &a, int bx, int by) {
     const Geo &g = a.g;
-    const int nh = blockIdx.x * blockDim.x + threadIdx.x, n = blockIdx.y;
+    const int nh = bx * blockDim.x + threadIdx.x, n = by;
     if (nh >= g.H) return;
     const size_t at = (size_t)n * g.Hp + nh;
     if (n == 0 || n == g.N - 1) {
@@ -323,19 +326,19 @@ __global__ void k_step_proj(StepArgs a) {
 
 // S4: warp = one (system, re/im) of 32 consecutive modes; the pivot-free
 // sweep is used for the systems whose factorisation did not pivot
-__global__ void __launch_bounds__(192) k_solve_ld(StepArgs a) {
+__device__ __forceinline__ void solve_ld_body(const StepArgs &a, int bx) {
     extern __shared__ double ring4[];
     const Geo &g = a.g;
     const int w = threadIdx.x >> 5;
-    const int nh = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int nh = bx * 32 + (threadIdx.x & 31);
     const int sys = w >> 1, part = w & 1;
     if (nh >= g.H) return;
     const size_t st = 2 * (size_t)g.Hp;
-    const double *rhs = reinterpret_cast<const double *>(a.rl[sys]) + 2 * (size_t)nh + part;
-    double *out = reinterpret_cast<double *>(a.v[sys]) + 2 * (size_t)nh + part;
+    const double *rhs = reinterpret_cast<const double *>(pick3(a.rl, sys)) + 2 * (size_t)nh + part;
+    double *out = reinterpret_cast<double *>(pick3(a.v, sys)) + 2 * (size_t)nh + part;
     const double *lu = sys == 0 ? a.ldp : sys == 1 ? a.ldm : a.ldz;
-    if (a.ldpiv[sys])  // pivoting band (low Re, small dt or very clustered meshes)
-        solve_async<true>(lu, a.pivld[sys], g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x, blockDim.x);
+    if (pick3(a.ldpiv, sys))  // pivoting band (low Re, small dt or very clustered meshes)
+        solve_async<true>(lu, pick3(a.pivld, sys), g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x, blockDim.x);
     else
         solve_async<false>(lu, nullptr, g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x, blockDim.x);
 }
@@ -343,14 +346,14 @@ __global__ void __launch_bounds__(192) k_solve_ld(StepArgs a) {
 // ------------------------------------------------------------------- S5
 __device__ __forceinline__ double sq(double2 a) { return a.x * a.x + a.y * a.y; }
 
-__global__ void __launch_bounds__(TM *TR) k_step_final(StepArgs a) {
+__device__ __forceinline__ void step_final_body(const StepArgs &a, int bx) {
     __shared__ double coef[TM][8];        // aR(1..4), aI(1..4) per mode
     __shared__ double red[TM * TR];
     __shared__ double m0buf[3][2][128];    // mode 0 after pm2rt (N <= 128)
     const Geo &g = a.g;
     const int N = g.N, Hp = g.Hp;
     const int tx = threadIdx.x % TM, ty = threadIdx.x / TM;
-    const int nh = blockIdx.x * TM + tx;
+    const int nh = bx * TM + tx;
     const bool live = nh < g.H;
     int k = 0, m = 0;
     if (live) mode_km(nh, g.K, k, m);
@@ -429,7 +432,7 @@ __global__ void __launch_bounds__(TM *TR) k_step_final(StepArgs a) {
             a.u[2][at] = z;
         }
     }
-    if (blockIdx.x == 0) {  // mode 0: flux adjustment and symmetry zeros
+    if (bx == 0) {  // mode 0: flux adjustment and symmetry zeros
         __syncthreads();
         double s = 0.0;
         for (int n = threadIdx.x; n < N; n += blockDim.x) s += m0buf[2][0][n] * a.dm.intrdr[n];
@@ -469,19 +472,36 @@ __global__ void __launch_bounds__(TM *TR) k_step_final(StepArgs a) {
     }
 }
 
+// ------------------------------------------------------------- kernels
+// Lone pipe: one launch per stage over that pipe's tiles.  Batch: one launch
+// per stage over the tiles of every pipe, blk[b] = (pipe, tile of that pipe).
+__global__ void __launch_bounds__(TM *TR) k_step_rhs(StepArgs a) { step_rhs_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(64) k_solve_pnp(StepArgs a) { solve_pnp_body(a, blockIdx.x); }
+__global__ void k_step_proj(StepArgs a) { step_proj_body(a, blockIdx.x, blockIdx.y); }
+__global__ void __launch_bounds__(192) k_solve_ld(StepArgs a) { solve_ld_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(TM *TR) k_step_final(StepArgs a) { step_final_body(a, blockIdx.x); }
+
+#define PF_BATCH1(NAME, BODY, BOUNDS)                                                          \
+    __global__ void BOUNDS NAME(const StepArgs *__restrict__ args, const int2 *__restrict__ blk) { \
+        const int2 pb = blk[blockIdx.x];                                                       \
+        const StepArgs a = args[pb.x]; /* by value: stores cannot alias it */                  \
+        BODY(a, pb.y);                                                                         \
+    }
+PF_BATCH1(k_step_rhs_batch, step_rhs_body, __launch_bounds__(TM *TR))
+PF_BATCH1(k_solve_pnp_batch, solve_pnp_body, __launch_bounds__(64))
+PF_BATCH1(k_solve_ld_batch, solve_ld_body, __launch_bounds__(192))
+PF_BATCH1(k_step_final_batch, step_final_body, __launch_bounds__(TM *TR))
+#undef PF_BATCH1
+
+__global__ void __launch_bounds__(128) k_step_proj_batch(const StepArgs *__restrict__ args, const int2 *__restrict__ blk) {
+    const int2 pb = blk[blockIdx.x];
+    const StepArgs a = args[pb.x];
+    const int gx = (a.g.H + 127) / 128;
+    step_proj_body(a, pb.y % gx, pb.y / gx);
+}
+
 // ------------------------------------------------------------------ host
-// One predictor (corrector=0) or corrector (corrector=1) vel_step.  The
-// predictor's u_ := u copy is a pointer swap of vel[0..2] and prev[0..2].
-int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
-    const Geo &g = ctx->g;
-    if (g.N > TR * 16 || g.N > 128) {
-        pf_set_error("fused step supports N <= 128");
-        return PF_ERR_ARG;
-    }
-    if (!corrector) {
-        for (int i = 0; i < 3; ++i) std::swap(ctx->vel[i].d, ctx->prev[i].d);
-        ctx->parity ^= 1;
-    }
+static StepArgs make_step_args(const pf_ctx *ctx, int corrector) {
     StepArgs a;
     for (int i = 0; i < 3; ++i) {
         a.u_[i] = ctx->prev[i].d;
@@ -498,13 +518,10 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
     a.lnp = ctx->LNp.lu;
     a.pivd = ctx->LNp.pivd;
     const pf_lumesh *ld[3] = {&ctx->LDp, &ctx->LDm, &ctx->LDz};
-    bool anyld = false;
     for (int i = 0; i < 3; ++i) {
         a.pivld[i] = ld[i]->pivd;
         a.ldpiv[i] = ld[i]->pivoted;
-        anyld |= ld[i]->pivoted != 0;
     }
-    const int ldsw = anyld ? KV + 1 : KL + 1;  // ring slot width of the Helmholtz solves
     a.ldp = ctx->LDp.lu;
     a.ldm = ctx->LDm.lu;
     a.ldz = ctx->LDz.lu;
@@ -512,22 +529,52 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
     a.Ainv = ctx->Ainv;
     a.Ui = ctx->Ui;
     a.dm = ctx->dm;
-    a.g = g;
+    a.g = ctx->g;
     a.c1 = ctx->Ltz.c1;
     a.c2 = ctx->Ltz.c2;
     a.implicit = ctx->cfg.implicit;
     a.mode = corrector;
     a.const_flux = ctx->cfg.const_flux;
     a.sc = ctx->dsc;
-    const unsigned tiles = grid1(g.H, TM);
+    return a;
+}
+
+static bool any_ld_pivoted(const pf_ctx *ctx) {
+    return ctx->LDp.pivoted || ctx->LDm.pivoted || ctx->LDz.pivoted;
+}
+
+static int step_attrs() {
     static bool attrs_set = false;
     if (!attrs_set) {
-        PF_CUDA(cudaFuncSetAttribute(k_solve_ld, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(192 * RING * (KV + 1) * sizeof(double))));
-        PF_CUDA(cudaFuncSetAttribute(k_solve_pnp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(64 * RING * (KV + 1) * sizeof(double))));
+        const int ld = (int)(192 * RING * (KV + 1) * sizeof(double));
+        const int pnp = (int)(64 * RING * (KV + 1) * sizeof(double));
+        PF_CUDA(cudaFuncSetAttribute(k_solve_ld, cudaFuncAttributeMaxDynamicSharedMemorySize, ld));
+        PF_CUDA(cudaFuncSetAttribute(k_solve_pnp, cudaFuncAttributeMaxDynamicSharedMemorySize, pnp));
+        PF_CUDA(cudaFuncSetAttribute(k_solve_ld_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, ld));
+        PF_CUDA(cudaFuncSetAttribute(k_solve_pnp_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, pnp));
         attrs_set = true;
     }
+    return PF_OK;
+}
+
+static bool pf_fused_step_geo_ok(const Geo &g) { return g.N <= TR * 16 && g.N <= 128; }
+
+// One predictor (corrector=0) or corrector (corrector=1) vel_step.  The
+// predictor's u_ := u copy is a pointer swap of vel[0..2] and prev[0..2].
+int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
+    const Geo &g = ctx->g;
+    if (!pf_fused_step_geo_ok(g)) {
+        pf_set_error("fused step supports N <= 128");
+        return PF_ERR_ARG;
+    }
+    if (!corrector) {
+        for (int i = 0; i < 3; ++i) std::swap(ctx->vel[i].d, ctx->prev[i].d);
+        ctx->parity ^= 1;
+    }
+    const StepArgs a = make_step_args(ctx, corrector);
+    const int ldsw = any_ld_pivoted(ctx) ? KV + 1 : KL + 1;  // ring slot width of the Helmholtz solves
+    const unsigned tiles = grid1(g.H, TM);
+    PF_TRY(step_attrs());
     {
         ProfScope ps_(ctx, PF_K_STEP);
         k_step_rhs<<<tiles, TM * TR, (size_t)g.N * TM * sizeof(double2), ctx->stream>>>(a);
@@ -548,11 +595,117 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
         k_solve_ld<<<tiles, 192, (size_t)192 * RING * ldsw * sizeof(double), ctx->stream>>>(a);
     }
     PF_LAUNCHED(ctx);
-    if (corrector) PF_CUDA(cudaMemsetAsync(&ctx->dsc->dterr2_bits, 0, sizeof(unsigned long long), ctx->stream));
     {
         ProfScope ps_(ctx, PF_K_INFL);
         k_step_final<<<tiles, TM * TR, 0, ctx->stream>>>(a);
     }
     PF_LAUNCHED(ctx);
+    return PF_OK;
+}
+
+// ---------------------------------------------------------------- batched
+// Step arguments of every pipe for both pointer parities and both modes,
+// and the tile maps of the five stages.
+struct pf_step_batch {
+    int n;
+    StepArgs *d_args[2][2];  // [pointer state after the predictor's swap][mode]
+    int2 *tile, *proj;       // (pipe, tile) maps: 32-mode tiles, 128-mode x row tiles
+    int ntile, nproj;
+    int maxN;
+    bool anypiv;
+};
+
+void pf_step_batch_free(pf_step_batch *b) {
+    if (!b) return;
+    for (int s = 0; s < 2; ++s)
+        for (int m = 0; m < 2; ++m) cudaFree(b->d_args[s][m]);
+    cudaFree(b->tile);
+    cudaFree(b->proj);
+    delete b;
+}
+
+// state 0: the pointers as the pipes hold them now; state 1: vel/prev swapped
+int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
+    *out = nullptr;
+    pf_step_batch *b = new pf_step_batch();
+    b->n = n;
+    b->maxN = 0;
+    b->anypiv = false;
+    std::vector<StepArgs> h(n);
+    std::vector<int2> tile, proj;
+    for (int i = 0; i < n; ++i) {
+        const Geo &g = pipes[i]->g;
+        if (!pf_fused_step_geo_ok(g)) {
+            pf_step_batch_free(b);
+            pf_set_error("batched step supports N <= 128");
+            return PF_ERR_ARG;
+        }
+        b->maxN = std::max(b->maxN, g.N);
+        b->anypiv |= any_ld_pivoted(pipes[i]);
+        for (int t = 0; t < (int)grid1(g.H, TM); ++t) tile.push_back(make_int2(i, t));
+        for (int t = 0; t < (int)grid1(g.H, 128) * g.N; ++t) proj.push_back(make_int2(i, t));
+    }
+    for (int s = 0; s < 2; ++s)
+        for (int m = 0; m < 2; ++m) {
+            for (int i = 0; i < n; ++i) {
+                pf_ctx *c = pipes[i];
+                if (s) for (int k = 0; k < 3; ++k) std::swap(c->vel[k].d, c->prev[k].d);
+                h[i] = make_step_args(c, m);
+                if (s) for (int k = 0; k < 3; ++k) std::swap(c->vel[k].d, c->prev[k].d);
+            }
+            if (cudaMalloc((void **)&b->d_args[s][m], n * sizeof(StepArgs)) != cudaSuccess ||
+                cudaMemcpy(b->d_args[s][m], h.data(), n * sizeof(StepArgs), cudaMemcpyHostToDevice) != cudaSuccess) {
+                pf_step_batch_free(b);
+                pf_set_error("batched step: argument upload failed");
+                return PF_ERR_CUDA;
+            }
+        }
+    b->ntile = (int)tile.size();
+    b->nproj = (int)proj.size();
+    if (cudaMalloc((void **)&b->tile, tile.size() * sizeof(int2)) != cudaSuccess ||
+        cudaMalloc((void **)&b->proj, proj.size() * sizeof(int2)) != cudaSuccess ||
+        cudaMemcpy(b->tile, tile.data(), tile.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->proj, proj.data(), proj.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess) {
+        pf_step_batch_free(b);
+        pf_set_error("batched step: tile map upload failed");
+        return PF_ERR_CUDA;
+    }
+    *out = b;
+    return PF_OK;
+}
+
+// One predictor or corrector vel_step of every pipe in five launches; the
+// caller tracks the pointer state (the predictor's swap is the caller's).
+int pf_step_batch_launch(pf_step_batch *b, int state, int corrector, cudaStream_t st, pf_stage_prof *prof,
+                         unsigned long long *nk) {
+    PF_TRY(step_attrs());
+    const StepArgs *a = b->d_args[state][corrector ? 1 : 0];
+    const int ldsw = b->anypiv ? KV + 1 : KL + 1;
+    {
+        StageScope ss_(prof, PF_K_STEP, st);
+        k_step_rhs_batch<<<b->ntile, TM * TR, (size_t)b->maxN * TM * sizeof(double2), st>>>(a, b->tile);
+    }
+    PF_CHECK_LAUNCH();
+    {
+        StageScope ss_(prof, PF_K_LUSOLVE, st);
+        k_solve_pnp_batch<<<b->ntile, 64, (size_t)64 * RING * (KV + 1) * sizeof(double), st>>>(a, b->tile);
+    }
+    PF_CHECK_LAUNCH();
+    {
+        StageScope ss_(prof, PF_K_STEP, st);
+        k_step_proj_batch<<<b->nproj, 128, 0, st>>>(a, b->proj);
+    }
+    PF_CHECK_LAUNCH();
+    {
+        StageScope ss_(prof, PF_K_LUSOLVE, st);
+        k_solve_ld_batch<<<b->ntile, 192, (size_t)192 * RING * ldsw * sizeof(double), st>>>(a, b->tile);
+    }
+    PF_CHECK_LAUNCH();
+    {
+        StageScope ss_(prof, PF_K_INFL, st);
+        k_step_final_batch<<<b->ntile, TM * TR, 0, st>>>(a, b->tile);
+    }
+    PF_CHECK_LAUNCH();
+    *nk += 5;
     return PF_OK;
 }

@@ -130,6 +130,8 @@ _SIGS = {
     "pf_batch_stream": [P, PP],
     "pf_batch_prof_enable": [P, I],
     "pf_batch_prof_read": [P, I, DP, C.POINTER(C.c_ulonglong)],
+    "pf_batch_launches": [P, C.POINTER(C.c_ulonglong)],
+    "pf_batch_staged": [P, C.POINTER(I)],
     "pf_ctx_launches": [P, C.POINTER(C.c_ulonglong)],
     "pf_prof_enable": [P, I],
     "pf_prof_read": [P, I, DP, C.POINTER(C.c_ulonglong)],

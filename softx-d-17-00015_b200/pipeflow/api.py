@@ -493,7 +493,8 @@ class Pipe:
 
 class Batch:
     """Independent pipes of uneven size advanced together (pf_batch_*): one
-    CUDA graph per batch timestep, one kernel chain per pipe."""
+    CUDA graph per batch timestep, each stage launched once over all pipes
+    where the pipes allow it, else one kernel chain per pipe."""
 
     def __init__(self, cfgs, device: int = -1):
         self.lib = L.load()
@@ -544,6 +545,18 @@ class Batch:
             _check(self.lib.pf_batch_prof_read(self.h, i, C.byref(ms), C.byref(n)))
             out[name] = (ms.value, n.value)
         return out
+
+    def launches(self) -> int:
+        """Kernels launched so far by the batch (the pipes' and the batched ones)."""
+        n = C.c_ulonglong()
+        _check(self.lib.pf_batch_launches(self.h, C.byref(n)))
+        return n.value
+
+    def staged(self) -> bool:
+        """True when each stage of a step is one launch over every pipe."""
+        v = C.c_int()
+        _check(self.lib.pf_batch_staged(self.h, C.byref(v)))
+        return bool(v.value)
 
     def close(self):
         if self.h:

@@ -21,9 +21,12 @@ UNEVEN = [
 ]
 
 
-def _cfgs(prec=0):
+PIVOTING = dict(N=64, K=4, M=4, Mp=1, Re=1900.0, alpha=1.25, dt=0.01)  # its Helmholtz factors pivot
+
+
+def _cfgs(prec=0, extra=()):
     import pipeflow as P
-    return [P.PipeConfig(**d, precision=prec) for d in UNEVEN]
+    return [P.PipeConfig(**d, precision=prec) for d in UNEVEN] + [P.PipeConfig(**d, precision=prec) for d in extra]
 
 
 def _seed(pipe, i):
@@ -31,10 +34,22 @@ def _seed(pipe, i):
     P.seeded_state(pipe, 100 + i, 1e-3)
 
 
-@pytest.mark.parametrize("orbit", [False, True], ids=["main", "orbit"])
-def test_batch_equals_lone_pipes(orbit):
+# (orbit, precision, extra pipes, stage-batched graphs expected)
+VARIANTS = {
+    "main": (False, 0, (), True),
+    "orbit": (True, 0, (), True),
+    "mixed": (False, 1, (), True),
+    "pivot": (False, 0, (PIVOTING,), True),
+    # a mirror-symmetric pipe keeps the batch on per-pipe graph branches
+    "branch": (False, 0, (dict(N=32, K=8, M=8, Mp=1, Re=2000.0, alpha=1.0, dt=0.01, mirrorsym=True),), False),
+}
+
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
+def test_batch_equals_lone_pipes(variant):
     import pipeflow as P
-    cfgs = _cfgs()
+    orbit, prec, extra, staged = VARIANTS[variant]
+    cfgs = _cfgs(prec, extra)
     batch = P.Batch(cfgs)
     batch.matrices()
     alone = [P.Pipe(c) for c in cfgs]
@@ -43,7 +58,10 @@ def test_batch_equals_lone_pipes(orbit):
         _seed(bp, i)
         _seed(ap, i)
     nsteps = 5
+    n0 = batch.launches()
     batch.step(nsteps, orbit=orbit)
+    assert batch.staged() == staged
+    assert batch.launches() > n0
     for ap in alone:
         if orbit:
             ap.steporbit(nsteps)
@@ -54,6 +72,28 @@ def test_batch_equals_lone_pipes(orbit):
         for (br, bi), (ar, ai) in zip(bp.get_state(), ap.get_state()):
             assert np.array_equal(br, ar) and np.array_equal(bi, ai)
         assert bp.tim.step == ap.tim.step == nsteps
+        assert bp.tim.dt == ap.tim.dt
+    batch.close()
+
+
+def test_batch_staged_launch_count():
+    """A stage-batched step is a fixed number of launches, whatever the pipe count."""
+    import pipeflow as P
+    batch = P.Batch(_cfgs())
+    batch.matrices()
+    for i, bp in enumerate(batch.pipes):
+        _seed(bp, i)
+    batch.step(1)  # eager first step
+    n0 = batch.launches()
+    passes = batch.step(2, orbit=True)
+    assert passes == 2 * len(batch.pipes)
+    assert batch.staged()
+    # per step: mean-mode symmetry, the transform stages (one launch per
+    # distinct length: zinv and zfwd by Z, theta by Th), 5 step stages, the
+    # transform stages again, 5 step stages, the symmetry again, scalar gather
+    cfgs = _cfgs()
+    nl = 2 * len({c.Z for c in cfgs}) + len({c.Th for c in cfgs})
+    assert batch.launches() - n0 == 2 * (1 + nl + 5 + nl + 5 + 1 + 1)
     batch.close()
 
 
