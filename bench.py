@@ -487,8 +487,14 @@ def main():
             "clocks": r["clk"],
         }
         if args.workload == "batched":
-            line["roofline"]["note"] = ("kernel spans of concurrent pipes overlap in time, so the per-launch "
-                                        "duration includes GPU sharing and frac is a lower bound")
+            if r["extra"].get("stage_batched"):
+                line["roofline"]["note"] = (
+                    "one launch covers every pipe; a category's launches of different transform lengths "
+                    "run concurrently and are timed as one span; algorithmic bytes exclude the LU factors "
+                    "and influence vectors that the solves stream (traffic includes them)")
+            else:
+                line["roofline"]["note"] = ("kernel spans of concurrent pipes overlap in time, so the per-launch "
+                                            "duration includes GPU sharing and frac is a lower bound")
         line.update(r["extra"])
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.workload, max(1, args.ref_steps))

@@ -314,3 +314,26 @@ def test_pivoting_helmholtz_fused_path_parity():
     o.vel_predictor()
     g.vel_predictor()
     assert O.rel_l2(state_from_dev(g), o.state()) <= 1e-12
+
+
+def test_adaptive_dt_parity():
+    """Variable dt (main.f90:24-29): vel_maxtstep, tim_new_tstep and the
+    re-factorisation on a dt change follow the oracle step for step."""
+    cfgd = dict(SMALL[0], dt=-1.0, maxdt=0.01, courant=0.5)
+    o, g = oracle_pipe(cfgd), device_pipe(cfgd)
+    o.tim_dt = 0.004
+    t = g.tim
+    t.dt = 0.004
+    g.set_tim(t)
+    o.vel_matrices()
+    g.vel_matrices()
+    st = O.seeded_state(o, 11, 1e-3)
+    o.set_state(*st)
+    state_to_dev(g, st)
+    dts = [g.tim.dt]
+    for _ in range(6):
+        assert o.timestep() == g.timestep()
+        assert abs(g.tim.dt - o.tim_dt) <= 1e-15 * o.tim_dt
+        dts.append(g.tim.dt)
+    assert len(set(dts)) > 1  # dt did change
+    assert O.rel_l2(state_from_dev(g), o.state()) <= 1e-12
