@@ -406,6 +406,8 @@ def run_batched(args, torch, P, dist, world, rank, local):
                                   f"through pf_timestep"}
         extra["batched_over_plain"] = (args.pipes * args.steps / (ms / 1e3)) / plain
         extra["mixed_vs_fp64"] = mixed_error(P, cfgs[0], seeds[0], args.err_steps)
+        if args.with_serve:
+            extra["serve"] = run_serve(args, P, local, plain)
         if args.with_cfg2:
             sub = argparse.Namespace(**vars(args))
             sub.workload, sub.spinup, sub.steps = "cfg2", args.cfg2_spinup, args.cfg2_steps
@@ -418,6 +420,34 @@ def run_batched(args, torch, P, dist, world, rank, local):
     return dict(ms=ms, e2e_ms=e2e_ms, ne=ne, count=args.pipes, launches=launches, clk=clk.summary(),
                 extra=extra, dom=dom, dom_ms=dom_ms, dom_n=dom_n, per_launch=per_launch, h2d=io, d2h=io,
                 dtype="mixed: f32 transforms, f64 solves", config=config_of(args))
+
+
+KRYLOV = dict(N=48, K=32, M=24, Mp=1, Re=2000.0, alpha=1.25)
+
+
+def run_serve(args, P, local, plain_value):
+    """Config-4 serving: Poisson arrivals of time-T-map requests (T uniform in
+    [1, 20], dt = 0.01), 30% GMRES Krylov-vector evaluations at N=48 K=32 M=24
+    (FP64, base state + 1e-7 seeded perturbation), the rest on the batched
+    mix's sizes in mixed precision; 150 GB HBM admission budget; continuous
+    batching.  The arrival window is bounded so the run takes seconds."""
+    from pipeflow import serve as S
+    reqs = S.make_stream(args.serve_rate, args.serve_window, 4, batched_configs(64), KRYLOV, device=local)
+    srv = P.Server(hbm_budget=150 * 10**9, device=local)
+    n0 = srv.launches()
+    makespan = S.run_stream(srv, reqs)
+    launches = srv.launches() - n0
+    srv.close()
+    out = S.latency_summary(reqs)
+    out.update({"rate_req_per_s": args.serve_rate, "arrival_window_s": args.serve_window,
+                "hbm_budget_bytes": 150 * 10**9, "makespan_s": makespan,
+                "served_timesteps_per_s": out["pipe_steps"] / makespan,
+                "served_over_plain": out["pipe_steps"] / makespan / plain_value,
+                "gpu_launches": launches,
+                "note": "latency from arrival to the result on the host; the offered load "
+                        f"({args.serve_rate:.0f} req/s x ~1050 steps each) exceeds one GPU's throughput, so "
+                        "every arrival joins a growing batch and latency grows with the number in flight"})
+    return out
 
 
 def main():
@@ -437,6 +467,9 @@ def main():
     ap.add_argument("--cfg2-steps", type=int, default=200)
     ap.add_argument("--no-cfg2", dest="with_cfg2", action="store_false")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-window", type=float, default=0.5)
+    ap.add_argument("--no-serve", dest="with_serve", action="store_false")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 

@@ -86,6 +86,11 @@ int pf_version(int *major, int *minor);
  * timestep.f90:29-40; velocity.f90:47-55).  device < 0 keeps the current one. */
 int pf_ctx_create(const pf_config *cfg, int device, pf_ctx **out);
 int pf_ctx_destroy(pf_ctx *ctx);
+/* New physical parameters (Re, alpha, dt, implicit, dterr, courant, maxdt,
+ * flags) for a context of the same N, K, M, Mp, precision and default mesh:
+ * the context starts a fresh run as pf_ctx_create would, reusing its device
+ * memory.  pf_vel_matrices must be called again before stepping. */
+int pf_ctx_reconfigure(pf_ctx *ctx, const pf_config *cfg);
 /* Run the context's work on an external cudaStream_t (NULL = own stream). */
 int pf_ctx_set_stream(pf_ctx *ctx, void *cuda_stream);
 int pf_ctx_sync(pf_ctx *ctx);
@@ -251,10 +256,53 @@ int pf_batch_stream(pf_batch *b, void **stream);
  * time, so per-launch durations here include the sharing of the GPU. */
 int pf_batch_prof_enable(pf_batch *b, int mask);
 int pf_batch_prof_read(pf_batch *b, int cat, double *ms, unsigned long long *launches);
+/* Number of pipes, and membership changes.  A batch made with npipes = 0
+ * starts empty.  pf_batch_attach adds a context the caller created and still
+ * owns (same device; it must outlive its membership); pf_batch_detach removes
+ * it.  The batch's launches are rebuilt at the next step. */
+int pf_batch_size(pf_batch *b, int *n);
+int pf_batch_attach(pf_batch *b, pf_ctx *c);
+int pf_batch_detach(pf_batch *b, pf_ctx *c);
+/* on = 1 (default): steps replay captured CUDA graphs; on = 0: every step
+ * launches its kernels directly (for membership that changes every step). */
+int pf_batch_set_graphs(pf_batch *b, int on);
 /* Kernels launched so far by the batch (its pipes' and its batched ones). */
 int pf_batch_launches(pf_batch *b, unsigned long long *n);
 /* *staged = 1 when the batch's graphs launch each stage once for all pipes. */
 int pf_batch_staged(pf_batch *b, int *staged);
+
+/* ---------------------------------------------------------------- serving */
+/* Requests "advance this state by nsteps timesteps" (time-T maps, e.g. the
+ * Newton-Krylov evaluations of newton.f90:399-465 through steporbit,
+ * newton.f90:721-787) served with continuous batching: every admitted
+ * request's state stays resident in its own context, and all of them advance
+ * together in one batch (stage-batched launches).  Between batch steps the
+ * server admits queued requests in arrival order while the HBM budget and the
+ * slot cap allow (reusing pooled contexts of the same shape) and retires the
+ * finished ones.  A request's result equals the lone-pipe result exactly.
+ * No single reference routine: the reference runs one state per process. */
+typedef struct pf_server pf_server;
+/* orbit = 1: steporbit steps (one corrector each); 0: main-loop steps. */
+int pf_serve_create(int device, unsigned long long hbm_budget_bytes, int max_active, int orbit,
+                    pf_server **out);
+int pf_serve_destroy(pf_server *s);
+/* Queue a request (cfg->dt > 0, default mesh); the six arrays (reference coll
+ * layout, H*N doubles each) are copied. */
+int pf_serve_submit(pf_server *s, const pf_config *cfg, int nsteps,
+                    const double *ur_re, const double *ur_im, const double *ut_re,
+                    const double *ut_im, const double *uz_re, const double *uz_im, long long *id);
+/* Admit what fits, advance every admitted request one timestep, retire the
+ * finished; *admitted / *finished (may be NULL) count this call's. */
+int pf_serve_step(pf_server *s, int *admitted, int *finished);
+/* Ids finished since the last call (up to cap). */
+int pf_serve_finished(pf_server *s, long long *ids, int cap, int *n);
+/* Final state of a finished request; the request is forgotten afterwards. */
+int pf_serve_result(pf_server *s, long long id, double *ur_re, double *ur_im, double *ut_re,
+                    double *ut_im, double *uz_re, double *uz_im);
+int pf_serve_stats(pf_server *s, int *queued, int *active, int *pooled, unsigned long long *bytes,
+                   long long *steps);
+/* The batch the server steps (its stream, launch counter and profiling). */
+int pf_serve_batch(pf_server *s, pf_batch **b);
 
 /* ------------------------------------------------------- instrumentation */
 /* Kernel categories timed by CUDA events when profiling is on (the reference

@@ -47,14 +47,17 @@ __global__ void k_batch_scalars(DevScalars *const *__restrict__ src, DevScalars 
 struct pf_batch {
     int n;
     std::vector<pf_ctx *> pipes;
+    std::vector<char> owned;   // created (and destroyed) by the batch, or attached by the caller
+    int device;
     cudaStream_t master;
     cudaEvent_t fork;
     std::vector<cudaEvent_t> join;
-    cudaGraphExec_t g[2][2];   // [orbit][parity]
+    cudaGraphExec_t g[2][2];   // [orbit][parity of pipe 0]
     unsigned long long gn[2][2];
-    int parity;
-    bool warm;
+    bool warm;                 // the per-pipe eager step has run (branch graphs)
+    bool use_graphs;           // capture steps into graphs (else launch directly)
     DevScalars *hsc;           // pinned, one per pipe
+    int hsc_cap;
     // event pairs of profiled categories captured into each graph:
     // (pipe, category, start, stop)
     struct Ev {
@@ -63,12 +66,15 @@ struct pf_batch {
     };
     std::vector<Ev> gev[2][2];
     std::vector<unsigned long long> gnp[2][2];  // kernels per pipe in each graph
+    // graph form, decided when the first graph of a membership is made
+    int kind;                        // 0 undecided, 1 stage-batched, 2 per-pipe branches
+    std::vector<int> rel0;           // each pipe's pointer parity relative to pipe 0 then
+    unsigned long long gen0;         // sum of the pipes' matrices generations then
     // stage-batched launches
-    bool staged;                     // the graphs are stage-batched
+    bool fresh;                      // built, no step run yet (the first runs uncaptured)
     pf_nl_batch *nlb;
     pf_step_batch *stb;
-    int par0;                        // the pipes' pointer parity when nlb/stb were built
-    unsigned long long gen0;         // sum of the pipes' matrices generations then
+    int par0;                        // pipe 0's pointer parity when nlb/stb were built
     SymArgs *d_sym[2];               // [pointer state]
     DevScalars **d_scp;              // each pipe's device scalars
     DevScalars *d_scall;             // gathered scalars
@@ -117,11 +123,13 @@ static void batch_graphs_reset(pf_batch *b) {
             b->sev[o][p].clear();
         }
     staged_free(b);
-    b->staged = false;
+    b->kind = 0;
+    b->fresh = false;
+    b->warm = false;
 }
 
 static void batch_free(pf_batch *b) {
-    if (!b->pipes.empty()) batch_graphs_reset(b);
+    batch_graphs_reset(b);
     for (cudaEvent_t e : b->join) cudaEventDestroy(e);
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->master) cudaStreamDestroy(b->master);
@@ -131,38 +139,65 @@ static void batch_free(pf_batch *b) {
         b->sprof.pool.push_back(e.b);
     }
     for (cudaEvent_t e : b->sprof.pool) cudaEventDestroy(e);
-    for (pf_ctx *c : b->pipes) pf_ctx_destroy(c);
+    for (int i = 0; i < b->n; ++i)
+        if (b->owned[i]) pf_ctx_destroy(b->pipes[i]);
     delete b;
 }
 
+// per-pipe host resources for n pipes: join events and the pinned scalars
+static int batch_reserve(pf_batch *b, int n) {
+    while ((int)b->join.size() < n) {
+        cudaEvent_t e = nullptr;
+        PF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        b->join.push_back(e);
+    }
+    if (n > b->hsc_cap) {
+        const int cap = std::max(n, 2 * b->hsc_cap);
+        DevScalars *h = nullptr;
+        PF_CUDA(cudaMallocHost((void **)&h, cap * sizeof(DevScalars)));
+        if (b->hsc) cudaFreeHost(b->hsc);
+        b->hsc = h;
+        b->hsc_cap = cap;
+    }
+    return PF_OK;
+}
+
 extern "C" int pf_batch_create(int npipes, const pf_config *cfgs, int device, pf_batch **out) {
-    PF_ARG(npipes > 0 && cfgs && out, "pf_batch_create: bad argument");
+    PF_ARG(npipes >= 0 && (cfgs || npipes == 0) && out, "pf_batch_create: bad argument");
     *out = nullptr;
     pf_batch *b = new pf_batch();
-    b->n = npipes;
+    b->use_graphs = true;
+    if (device >= 0 && cudaSetDevice(device) != cudaSuccess) {
+        delete b;
+        pf_set_error("pf_batch_create: cannot select device %d", device);
+        return PF_ERR_NODEVICE;
+    }
+    if (cudaGetDevice(&b->device) != cudaSuccess) {
+        delete b;
+        pf_set_error("pf_batch_create: no CUDA device");
+        return PF_ERR_NODEVICE;
+    }
     for (int i = 0; i < npipes; ++i) {
         pf_ctx *c = nullptr;
-        const int s = pf_ctx_create(&cfgs[i], device, &c);
+        const int s = pf_ctx_create(&cfgs[i], b->device, &c);
         if (s != PF_OK) {
             batch_free(b);
             return s;
         }
         b->pipes.push_back(c);
+        b->owned.push_back(1);
+        b->n = (int)b->pipes.size();
     }
     if (cudaStreamCreateWithFlags(&b->master, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaMallocHost((void **)&b->hsc, npipes * sizeof(DevScalars)) != cudaSuccess) {
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) {
         batch_free(b);
-        pf_set_error("pf_batch_create: stream/event/pinned allocation failed");
+        pf_set_error("pf_batch_create: stream/event allocation failed");
         return PF_ERR_CUDA;
     }
-    b->join.resize(npipes);
-    for (int i = 0; i < npipes; ++i) {
-        if (cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) != cudaSuccess) {
-            batch_free(b);
-            pf_set_error("pf_batch_create: event creation failed");
-            return PF_ERR_CUDA;
-        }
+    const int s = batch_reserve(b, std::max(npipes, 1));
+    if (s != PF_OK) {
+        batch_free(b);
+        return s;
     }
     *out = b;
     return PF_OK;
@@ -176,6 +211,52 @@ extern "C" int pf_batch_destroy(pf_batch *b) {
 extern "C" int pf_batch_pipe(pf_batch *b, int i, pf_ctx **out) {
     PF_ARG(b && out && i >= 0 && i < b->n, "pf_batch_pipe: bad argument");
     *out = b->pipes[i];
+    return PF_OK;
+}
+
+extern "C" int pf_batch_size(pf_batch *b, int *n) {
+    PF_ARG(b && n, "pf_batch_size: bad argument");
+    *n = b->n;
+    return PF_OK;
+}
+
+// Add a context the caller owns (it must live on the batch's device and stay
+// alive until detached); the next step rebuilds the batch's launches.
+extern "C" int pf_batch_attach(pf_batch *b, pf_ctx *c) {
+    PF_ARG(b && c, "pf_batch_attach: bad argument");
+    PF_ARG(c->device == b->device, "pf_batch_attach: context is on another device");
+    for (pf_ctx *q : b->pipes) PF_ARG(q != c, "pf_batch_attach: context already in the batch");
+    batch_graphs_reset(b);
+    PF_TRY(batch_reserve(b, b->n + 1));
+    PF_CUDA(cudaStreamSynchronize(c->stream));  // its own pending work is done before batched launches
+    b->pipes.push_back(c);
+    b->owned.push_back(0);
+    b->n = (int)b->pipes.size();
+    return PF_OK;
+}
+
+// Remove a context the caller attached (the batch's own pipes stay).
+extern "C" int pf_batch_detach(pf_batch *b, pf_ctx *c) {
+    PF_ARG(b && c, "pf_batch_detach: bad argument");
+    for (int i = 0; i < b->n; ++i)
+        if (b->pipes[i] == c) {
+            PF_ARG(!b->owned[i], "pf_batch_detach: the batch owns this pipe");
+            batch_graphs_reset(b);
+            b->pipes.erase(b->pipes.begin() + i);
+            b->owned.erase(b->owned.begin() + i);
+            b->n = (int)b->pipes.size();
+            return PF_OK;
+        }
+    pf_set_error("pf_batch_detach: context not in the batch");
+    return PF_ERR_ARG;
+}
+
+// on = 1 (default): steps replay captured graphs; 0: every step launches
+// directly (for batches whose membership changes from step to step).
+extern "C" int pf_batch_set_graphs(pf_batch *b, int on) {
+    PF_ARG(b, "null batch");
+    if (!on) batch_graphs_reset(b);
+    b->use_graphs = on != 0;
     return PF_OK;
 }
 
@@ -196,8 +277,7 @@ static bool batch_graphable(const pf_batch *b) {
 // Whether the stage-batched kernels cover every pipe of the batch.
 static bool batch_stageable(const pf_batch *b) {
     for (const pf_ctx *c : b->pipes)
-        if (c->cfg.mirrorsym || c->cfg.shiftrefl || c->cfg.shiftrott || c->parity != b->pipes[0]->parity)
-            return false;
+        if (c->cfg.mirrorsym || c->cfg.shiftrefl || c->cfg.shiftrott) return false;
     return pf_nl_batch_supported(b->pipes.data(), b->n);
 }
 
@@ -351,6 +431,65 @@ static int batch_capture(pf_batch *b, int orbit, int par, cudaGraphExec_t *exec,
     return PF_OK;
 }
 
+// The pipes' pointer parities relative to pipe 0.  Every batched step swaps
+// every pipe, so they stay fixed unless a pipe is stepped on its own.
+static std::vector<int> rel_parity(const pf_batch *b) {
+    std::vector<int> r(b->n);
+    for (int i = 0; i < b->n; ++i) r[i] = b->pipes[i]->parity ^ b->pipes[0]->parity;
+    return r;
+}
+
+// Corrector control after a batched step (timestep.f90:214-253, main.f90:35-41)
+// from the scalars the step left in b->hsc; returns the passes taken.
+static long long batch_after_step(pf_batch *b, int orbit, int *status) {
+    long long passes = 0;
+    for (int i = 0; i < b->n; ++i) {
+        pf_ctx *c = b->pipes[i];
+        c->tim.dterr = std::max(c->tim.dterr, std::sqrt(bits_to_double(b->hsc[i].dterr2_bits)));
+        c->tim.it = 1;
+        int s = pf_tim_check_cgce(c);
+        ++passes;
+        if (!orbit) {
+            while (c->tim.it != 0) {  // further corrector passes for this pipe only
+                int e = pf_transform_nonlinear(c);
+                if (e == PF_OK) e = pf_vel_step_fused(c, 1);
+                if (e == PF_OK) e = pf_read_dterr(c);
+                if (e != PF_OK) {
+                    *status = e;
+                    c->tim.it = 0;
+                    break;
+                }
+                s = pf_tim_check_cgce(c);
+                ++passes;
+            }
+            if (s != PF_OK) *status = s;
+        } else {
+            c->tim.it = 0;
+        }
+        c->tim.t = c->tim.t + c->tim.dt;
+        c->tim.step = c->tim.step + 1;
+    }
+    return passes;
+}
+
+// Read the stage and kernel event pairs of a finished step into the totals.
+static void batch_collect_events(pf_batch *b, std::vector<pf_stage_prof::Open> *stage, bool release) {
+    for (auto &e : *stage) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
+            b->sprof.ms[e.cat] += ms;
+            b->sprof.n[e.cat] += 1;
+        } else {
+            cudaGetLastError();
+        }
+        if (release) {
+            b->sprof.pool.push_back(e.a);
+            b->sprof.pool.push_back(e.b);
+        }
+    }
+    if (release) stage->clear();
+}
+
 // Advance every pipe by nsteps timesteps.  orbit=0: the main.f90 step with
 // the corrector iterated to convergence per pipe; orbit=1: steporbit's step
 // with exactly one corrector.  *corr_passes (may be NULL) returns the total
@@ -360,8 +499,56 @@ extern "C" int pf_batch_step(pf_batch *b, int nsteps, int orbit, long long *corr
     orbit = orbit ? 1 : 0;
     long long passes = 0;
     int status = PF_OK;
-    for (int st = 0; st < nsteps; ++st) {
-        if (!b->warm || !batch_graphable(b)) {
+    for (int st = 0; st < nsteps && b->n > 0; ++st) {
+        if (!batch_graphable(b)) {  // adaptive dt, very large N, unbuilt lengths: eager per pipe
+            for (pf_ctx *c : b->pipes) {
+                if (orbit) {
+                    PF_TRY(pf_steporbit(c, 1));
+                    passes += 1;
+                } else {
+                    int nc = 0;
+                    const int s = pf_timestep(c, &nc);
+                    if (s != PF_OK) status = s;
+                    passes += nc;
+                }
+            }
+            continue;
+        }
+        // the graphs and batched arguments bake in each pipe's factor sets,
+        // 1/dt and pointer state relative to the other pipes
+        if (b->kind != 0 && (matrices_gen(b) != b->gen0 || rel_parity(b) != b->rel0)) batch_graphs_reset(b);
+        if (b->kind == 0) {
+            b->gen0 = matrices_gen(b);
+            b->rel0 = rel_parity(b);
+            b->kind = batch_stageable(b) ? 1 : 2;
+            if (b->kind == 1) {
+                PF_TRY(staged_build(b));
+                b->fresh = true;
+            }
+        }
+        const int p = b->pipes[0]->parity;
+        if (b->kind == 1 && (b->fresh || !b->use_graphs)) {
+            // launched directly: the first step after a build (it also sets
+            // the kernels' shared-memory limits outside any capture) and
+            // every step of a batch whose membership keeps changing
+            unsigned long long nk = 0;
+            const size_t open0 = b->sprof.open.size();
+            PF_TRY(staged_body(b, orbit, p, &nk));
+            b->launches += nk;
+            b->fresh = false;
+            for (pf_ctx *c : b->pipes) {
+                for (int i = 0; i < 3; ++i) std::swap(c->vel[i].d, c->prev[i].d);
+                c->parity ^= 1;
+                c->cfl_fused = true;
+            }
+            PF_CUDA(cudaStreamSynchronize(b->master));
+            std::vector<pf_stage_prof::Open> mine(b->sprof.open.begin() + open0, b->sprof.open.end());
+            b->sprof.open.resize(open0);
+            batch_collect_events(b, &mine, true);
+            passes += batch_after_step(b, orbit, &status);
+            continue;
+        }
+        if (b->kind == 2 && !b->warm) {
             // eager step per pipe (also sets every kernel attribute before any capture)
             for (pf_ctx *c : b->pipes) {
                 if (orbit) {
@@ -375,23 +562,11 @@ extern "C" int pf_batch_step(pf_batch *b, int nsteps, int orbit, long long *corr
                 }
             }
             b->warm = true;
+            b->rel0 = rel_parity(b);
             continue;
         }
-        const int p = b->pipes[0]->parity;
-        for (pf_ctx *c : b->pipes)
-            if (c->parity != p) {
-                pf_set_error("pf_batch_step: pipes out of step (pointer parity differs)");
-                return PF_ERR_STATE;
-            }
-        // the graphs bake in each pipe's factor sets and 1/dt
-        if (matrices_gen(b) != b->gen0) batch_graphs_reset(b);
         if (!b->g[orbit][p]) {
-            if (!(b->g[0][0] || b->g[0][1] || b->g[1][0] || b->g[1][1])) {  // choose the graph kind
-                b->gen0 = matrices_gen(b);
-                b->staged = batch_stageable(b);
-                if (b->staged) PF_TRY(staged_build(b));
-            }
-            if (b->staged) PF_TRY(staged_capture(b, orbit, p, &b->g[orbit][p], &b->gn[orbit][p]));
+            if (b->kind == 1) PF_TRY(staged_capture(b, orbit, p, &b->g[orbit][p], &b->gn[orbit][p]));
             else PF_TRY(batch_capture(b, orbit, p, &b->g[orbit][p], &b->gn[orbit][p]));
         }
         PF_CUDA(cudaGraphLaunch(b->g[orbit][p], b->master));
@@ -400,20 +575,12 @@ extern "C" int pf_batch_step(pf_batch *b, int nsteps, int orbit, long long *corr
             c->parity ^= 1;
             c->cfl_fused = true;
         }
-        if (b->staged)
+        if (b->kind == 1)
             b->launches += b->gn[orbit][p];
         else
             for (int i = 0; i < b->n; ++i) b->pipes[i]->launches += b->gnp[orbit][p][i];
         PF_CUDA(cudaStreamSynchronize(b->master));
-        for (auto &e : b->sev[orbit][p]) {  // stage times of the batched launches
-            float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
-                b->sprof.ms[e.cat] += ms;
-                b->sprof.n[e.cat] += 1;
-            } else {
-                cudaGetLastError();
-            }
-        }
+        batch_collect_events(b, &b->sev[orbit][p], false);
         for (auto &e : b->gev[orbit][p]) {  // kernel times of the profiled categories
             float ms = 0.f;
             pf_ctx *c = b->pipes[e.pipe];
@@ -424,27 +591,7 @@ extern "C" int pf_batch_step(pf_batch *b, int nsteps, int orbit, long long *corr
                 cudaGetLastError();
             }
         }
-        for (int i = 0; i < b->n; ++i) {
-            pf_ctx *c = b->pipes[i];
-            c->tim.dterr = std::max(c->tim.dterr, std::sqrt(bits_to_double(b->hsc[i].dterr2_bits)));
-            c->tim.it = 1;
-            int s = pf_tim_check_cgce(c);
-            ++passes;
-            if (!orbit) {
-                while (c->tim.it != 0) {  // further corrector passes for this pipe only
-                    PF_TRY(pf_transform_nonlinear(c));
-                    PF_TRY(pf_vel_step_fused(c, 1));
-                    PF_TRY(pf_read_dterr(c));
-                    s = pf_tim_check_cgce(c);
-                    ++passes;
-                }
-                if (s != PF_OK) status = s;
-            } else {
-                c->tim.it = 0;
-            }
-            c->tim.t = c->tim.t + c->tim.dt;
-            c->tim.step = c->tim.step + 1;
-        }
+        passes += batch_after_step(b, orbit, &status);
     }
     if (corr_passes) *corr_passes = passes;
     return status;
@@ -503,7 +650,7 @@ extern "C" int pf_batch_launches(pf_batch *b, unsigned long long *n) {
 // every pipe), 0 for per-pipe graph branches or before the first graph.
 extern "C" int pf_batch_staged(pf_batch *b, int *staged) {
     PF_ARG(b && staged, "pf_batch_staged: bad argument");
-    *staged = b->staged ? 1 : 0;
+    *staged = b->kind == 1 ? 1 : 0;
     return PF_OK;
 }
 

@@ -127,6 +127,7 @@ static int ctx_init(pf_ctx *ctx, const pf_config *cfg, int device) {
     ctx->own_stream = true;
     ctx->cfg = *cfg;
     ctx->cfg.r = nullptr;
+    ctx->custom_mesh = cfg->r != nullptr;
     Geo &g = ctx->g;
     g.N = cfg->N;
     g.K = cfg->K;
@@ -230,6 +231,37 @@ extern "C" int pf_ctx_create(const pf_config *cfg, int device, pf_ctx **out) {
         return s;
     }
     *out = ctx;
+    return PF_OK;
+}
+
+// New physical parameters for an existing context of the same shape (N, K,
+// M, Mp, precision, default mesh): a fresh run as pf_ctx_create would start
+// it, reusing the device memory.  vel_matrices must be called again.
+extern "C" int pf_ctx_reconfigure(pf_ctx *ctx, const pf_config *cfg) {
+    PF_ARG(ctx && cfg, "pf_ctx_reconfigure: null argument");
+    PF_ARG(cfg->N == ctx->cfg.N && cfg->K == ctx->cfg.K && cfg->M == ctx->cfg.M && cfg->Mp == ctx->cfg.Mp &&
+               cfg->precision == ctx->cfg.precision && cfg->r == nullptr && !ctx->custom_mesh,
+           "pf_ctx_reconfigure: shape, precision or mesh differs");
+    PF_ARG(cfg->alpha != 0.0, "var_coll_norm: alpha=0");
+    PF_ARG(cfg->Re > 0.0, "pf_ctx_reconfigure: Re must be > 0");
+    PF_CUDA(cudaSetDevice(ctx->device));
+    PF_CUDA(cudaStreamSynchronize(ctx->stream));
+    pf_graphs_reset(ctx);
+    ctx->cfg = *cfg;
+    ctx->cfg.r = nullptr;
+    ctx->g.alpha = cfg->alpha;
+    ctx->g.Re = cfg->Re;
+    ctx->matrices_ready = false;
+    ctx->LNp_set = false;
+    ctx->cfl_fused = false;
+    // tim_precompute (timestep.f90:29-40)
+    std::memset(&ctx->tim, 0, sizeof(ctx->tim));
+    ctx->tim.dt = cfg->dt;
+    ctx->tim.pcn = -1;
+    ctx->lasterr = 1e99;
+    ctx->newdt_i = 0;
+    ctx->vel_nu = 1.0;
+    PF_CUDA(cudaMemsetAsync(ctx->dsc, 0, sizeof(DevScalars), ctx->stream));
     return PF_OK;
 }
 

@@ -156,6 +156,7 @@ struct pf_ctx {
     pf_lumesh LNp, LDp, LDm, LDz;
     pf_mesh Ltp, Ltm, Ltz;
     bool LNp_set, matrices_ready;
+    bool custom_mesh;  // built from a caller-supplied radial mesh
     unsigned long long matrices_gen;  // bumped by every vel_matrices
     double vel_nu;
     double *U;           // influence solutions [(c*N + n)*Hp + nh], c=0..5

@@ -522,20 +522,20 @@ __global__ void k_nl_mean64_batch(const NLArgs *__restrict__ args, const int2 *_
 namespace {
 struct NLGroup {
     int L;
+    bool mixed;  // float2 (mixed precision) or double2 transforms
     int2 *blk;
     int nblk;
     size_t smem;
 };
-constexpr int NLB_STAGES = 3;  // zinv, theta, zfwd
-constexpr int NLB_MAXG = 12;   // transform lengths built
+constexpr int NLB_STAGES = 3;   // zinv, theta, zfwd
+constexpr int NLB_MAXG = 24;    // (transform length, precision) pairs
 }  // namespace
 
 struct pf_nl_batch {
-    bool mixed;
     int n;
     NLArgs *d_args[2];  // [pointer state]: 0 = as built, 1 = vel/prev swapped
     std::vector<NLGroup> groups[NLB_STAGES];
-    int2 *mean_blk;
+    int2 *mean_blk;     // FP64 mean mode of the mixed-precision pipes
     int nmean;
     cudaStream_t aux[NLB_MAXG];
     cudaEvent_t fork[NLB_STAGES], join[NLB_STAGES][NLB_MAXG];
@@ -543,9 +543,8 @@ struct pf_nl_batch {
 
 bool pf_nl_batch_supported(pf_ctx *const *pipes, int n) {
     if (n <= 0) return false;
-    const int prec = pipes[0]->cfg.precision;
     for (int i = 0; i < n; ++i)
-        if (pipes[i]->cfg.precision != prec || !pf_nl_fused_supported(pipes[i])) return false;
+        if (!pf_nl_fused_supported(pipes[i])) return false;
     return true;
 }
 
@@ -570,52 +569,66 @@ template <typename T> static int upload(T **d, const std::vector<T> &h) {
     return PF_OK;
 }
 
-// blocks of stage st for the pipes whose length (Z or Th) is L, largest
-// pipes first
-template <typename C> static int nlb_groups(pf_nl_batch *b, pf_ctx *const *pipes, int n) {
+static bool is_mixed(const pf_ctx *c) { return c->cfg.precision == PF_PREC_MIXED; }
+
+template <typename C> static NLTiles<C> tiles_of(const Geo &g) { return nl_tiles<C>(g); }
+
+// blocks of stage st for the pipes of one (length, precision) group
+template <typename C>
+static void nlb_group_map(int st, int L, bool mixed, pf_ctx *const *pipes, int n, std::vector<int2> &map,
+                          size_t &smem) {
+    for (int i = 0; i < n; ++i) {
+        const Geo &g = pipes[i]->g;
+        if ((st == 1 ? g.Th : g.Z) != L || is_mixed(pipes[i]) != mixed) continue;
+        const NLTiles<C> t = tiles_of<C>(g);
+        int nb = 0;
+        if (st == 0) nb = ((g.M + t.MC - 1) / t.MC) * g.N * 6;
+        if (st == 1) nb = ((g.Z + t.ZC - 1) / t.ZC) * g.N;
+        if (st == 2) nb = ((g.M + t.MC - 1) / t.MC) * g.N * 3;
+        for (int l = 0; l < nb; ++l) map.push_back(make_int2(i, l));
+        smem = std::max(smem, st == 1 ? t.tsm : t.zsm);
+    }
+}
+
+// one group per (stage, transform length, precision), longest lengths first
+static int nlb_groups(pf_nl_batch *b, pf_ctx *const *pipes, int n) {
     for (int st = 0; st < NLB_STAGES; ++st) {
-        std::vector<int> lengths;
+        std::vector<std::pair<int, int>> keys;  // (L, mixed)
         for (int i = 0; i < n; ++i) {
-            const int L = st == 1 ? pipes[i]->g.Th : pipes[i]->g.Z;
-            if (std::find(lengths.begin(), lengths.end(), L) == lengths.end()) lengths.push_back(L);
+            const std::pair<int, int> k(st == 1 ? pipes[i]->g.Th : pipes[i]->g.Z, is_mixed(pipes[i]) ? 1 : 0);
+            if (std::find(keys.begin(), keys.end(), k) == keys.end()) keys.push_back(k);
         }
-        std::sort(lengths.begin(), lengths.end(), std::greater<int>());
-        for (int L : lengths) {
+        std::sort(keys.begin(), keys.end(), std::greater<std::pair<int, int>>());
+        if ((int)keys.size() > NLB_MAXG) {
+            pf_set_error("batched transforms: too many (length, precision) groups");
+            return PF_ERR_ARG;
+        }
+        for (const auto &k : keys) {
             std::vector<int2> map;
             size_t smem = 0;
-            for (int i = 0; i < n; ++i) {
-                const Geo &g = pipes[i]->g;
-                if ((st == 1 ? g.Th : g.Z) != L) continue;
-                const NLTiles<C> t = nl_tiles<C>(g);
-                int nb = 0;
-                if (st == 0) nb = ((g.M + t.MC - 1) / t.MC) * g.N * 6;
-                if (st == 1) nb = ((g.Z + t.ZC - 1) / t.ZC) * g.N;
-                if (st == 2) nb = ((g.M + t.MC - 1) / t.MC) * g.N * 3;
-                for (int l = 0; l < nb; ++l) map.push_back(make_int2(i, l));
-                smem = std::max(smem, st == 1 ? t.tsm : t.zsm);
-            }
-            NLGroup gr{L, nullptr, (int)map.size(), smem};
-            b->groups[st].push_back(gr);
+            if (k.second) nlb_group_map<float2>(st, k.first, true, pipes, n, map, smem);
+            else nlb_group_map<double2>(st, k.first, false, pipes, n, map, smem);
+            b->groups[st].push_back(NLGroup{k.first, k.second != 0, nullptr, (int)map.size(), smem});
             PF_TRY(upload(&b->groups[st].back().blk, map));
         }
     }
     std::vector<int2> mean;
     for (int i = 0; i < n; ++i)
-        for (int l = 0; l < pipes[i]->g.N; ++l) mean.push_back(make_int2(i, l));
+        if (is_mixed(pipes[i]))
+            for (int l = 0; l < pipes[i]->g.N; ++l) mean.push_back(make_int2(i, l));
     b->nmean = (int)mean.size();
     return upload(&b->mean_blk, mean);
 }
 
-// Arguments of every pipe in both pointer states, and the per-length maps.
+// Arguments of every pipe in both pointer states, and the per-group maps.
 int pf_nl_batch_build(pf_ctx *const *pipes, int n, pf_nl_batch **out) {
     *out = nullptr;
     if (!pf_nl_batch_supported(pipes, n)) {
-        pf_set_error("batched transforms: mixed precisions or a transform length not built");
+        pf_set_error("batched transforms: a transform length is not built");
         return PF_ERR_ARG;
     }
     pf_nl_batch *b = new pf_nl_batch();
     b->n = n;
-    b->mixed = pipes[0]->cfg.precision == PF_PREC_MIXED;
     int s = PF_OK;
     std::vector<NLArgs> h(n);
     for (int st = 0; st < 2 && s == PF_OK; ++st) {
@@ -626,13 +639,15 @@ int pf_nl_batch_build(pf_ctx *const *pipes, int n, pf_nl_batch **out) {
         }
         s = upload(&b->d_args[st], h);
     }
-    if (s == PF_OK) s = b->mixed ? nlb_groups<float2>(b, pipes, n) : nlb_groups<double2>(b, pipes, n);
+    if (s == PF_OK) s = nlb_groups(b, pipes, n);
+    int ng = 0;
+    for (int st = 0; st < NLB_STAGES; ++st) ng = std::max(ng, (int)b->groups[st].size());
     for (int st = 0; st < NLB_STAGES && s == PF_OK; ++st) {
         if (cudaEventCreateWithFlags(&b->fork[st], cudaEventDisableTiming) != cudaSuccess) s = PF_ERR_CUDA;
         for (size_t k = 0; k < b->groups[st].size() && s == PF_OK; ++k)
             if (cudaEventCreateWithFlags(&b->join[st][k], cudaEventDisableTiming) != cudaSuccess) s = PF_ERR_CUDA;
     }
-    for (int k = 0; k < NLB_MAXG && s == PF_OK; ++k)
+    for (int k = 1; k < ng && s == PF_OK; ++k)
         if (cudaStreamCreateWithFlags(&b->aux[k], cudaStreamNonBlocking) != cudaSuccess) s = PF_ERR_CUDA;
     if (s != PF_OK) {
         if (s == PF_ERR_CUDA) pf_set_error("batched transforms: allocation failed");
@@ -669,8 +684,7 @@ template <typename C> static int nlb_group_launch(int st, const NLGroup &gr, con
     return PF_OK;
 }
 
-// one stage: the first length on st, the others forked onto auxiliary streams
-template <typename C>
+// one stage: the first group on st, the others forked onto auxiliary streams
 static int nlb_stage(pf_nl_batch *b, int stage, const NLArgs *args, cudaStream_t st, unsigned long long *nk) {
     const std::vector<NLGroup> &gs = b->groups[stage];
     if (gs.size() > 1) {
@@ -678,7 +692,9 @@ static int nlb_stage(pf_nl_batch *b, int stage, const NLArgs *args, cudaStream_t
         for (size_t k = 1; k < gs.size(); ++k) PF_CUDA(cudaStreamWaitEvent(b->aux[k], b->fork[stage], 0));
     }
     for (size_t k = 0; k < gs.size(); ++k) {
-        PF_TRY(nlb_group_launch<C>(stage, gs[k], args, k ? b->aux[k] : st));
+        cudaStream_t s = k ? b->aux[k] : st;
+        if (gs[k].mixed) PF_TRY(nlb_group_launch<float2>(stage, gs[k], args, s));
+        else PF_TRY(nlb_group_launch<double2>(stage, gs[k], args, s));
         ++*nk;
     }
     for (size_t k = 1; k < gs.size(); ++k) {
@@ -688,31 +704,24 @@ static int nlb_stage(pf_nl_batch *b, int stage, const NLArgs *args, cudaStream_t
     return PF_OK;
 }
 
-template <typename C>
-static int nlb_launch(pf_nl_batch *b, int state, cudaStream_t st, pf_stage_prof *prof, unsigned long long *nk) {
+// vel_transform + vel_nonlinear of every pipe: one launch per stage and
+// (transform length, precision) group, plus the FP64 mean-mode launch when
+// any pipe is in mixed precision; launches are counted into *nk.  state 0:
+// the pointers the pipes held when the batch was built; 1: vel/prev swapped.
+int pf_nl_batch_launch(pf_nl_batch *b, int state, cudaStream_t st, pf_stage_prof *prof, unsigned long long *nk) {
     const NLArgs *args = b->d_args[state];
     const int cats[NLB_STAGES] = {PF_K_ZINV, PF_K_THFWD, PF_K_ZFWD};
     for (int stage = 0; stage < NLB_STAGES; ++stage) {
         StageScope ss_(prof, cats[stage], st);
-        PF_TRY(nlb_stage<C>(b, stage, args, st, nk));
+        PF_TRY(nlb_stage(b, stage, args, st, nk));
     }
-    return PF_OK;
-}
-
-// vel_transform + vel_nonlinear of every pipe: one launch per stage and
-// transform length (mixed precision adds the FP64 mean-mode launch), counted
-// into *nk.  state 0: the pointers the pipes held when the batch was built;
-// 1: vel/prev swapped.
-int pf_nl_batch_launch(pf_nl_batch *b, int state, cudaStream_t st, pf_stage_prof *prof, unsigned long long *nk) {
-    if (b->mixed) {
-        PF_TRY(nlb_launch<float2>(b, state, st, prof, nk));
+    if (b->nmean > 0) {
         {
             StageScope ss_(prof, PF_K_ZFWD, st);
-            k_nl_mean64_batch<<<b->nmean, 256, 0, st>>>(b->d_args[state], b->mean_blk);
+            k_nl_mean64_batch<<<b->nmean, 256, 0, st>>>(args, b->mean_blk);
         }
         PF_CHECK_LAUNCH();
         *nk += 1;
-        return PF_OK;
     }
-    return nlb_launch<double2>(b, state, st, prof, nk);
+    return PF_OK;
 }

@@ -5,5 +5,5 @@ C ABI, include/pipeflow_b200.h); this package is the host-side mirror of the
 reference's Fortran module API over that ABI.
 """
 from ._lib import PF_PREC_FP64, PF_PREC_MIXED, KL, load  # noqa: F401
-from .api import Batch, Coll, LUMesh, Mesh, Phys, Pipe, PipeConfig, PipeflowError  # noqa: F401
+from .api import Batch, Coll, LUMesh, Mesh, Phys, Pipe, PipeConfig, PipeflowError, Server  # noqa: F401
 from .ic import seeded_state, vector_potential_host  # noqa: F401

@@ -58,6 +58,7 @@ _SIGS = {
     "pf_version": [IP, IP],
     "pf_ctx_create": [C.POINTER(pf_config), I, PP],
     "pf_ctx_destroy": [P],
+    "pf_ctx_reconfigure": [P, C.POINTER(pf_config)],
     "pf_ctx_set_stream": [P, P],
     "pf_ctx_sync": [P],
     "pf_ctx_dims": [P, IP, IP, IP, IP],
@@ -131,6 +132,19 @@ _SIGS = {
     "pf_batch_prof_enable": [P, I],
     "pf_batch_prof_read": [P, I, DP, C.POINTER(C.c_ulonglong)],
     "pf_batch_launches": [P, C.POINTER(C.c_ulonglong)],
+    "pf_batch_size": [P, C.POINTER(I)],
+    "pf_batch_attach": [P, P],
+    "pf_batch_detach": [P, P],
+    "pf_batch_set_graphs": [P, I],
+    "pf_serve_create": [I, C.c_ulonglong, I, I, PP],
+    "pf_serve_destroy": [P],
+    "pf_serve_submit": [P, C.POINTER(pf_config), I, DP, DP, DP, DP, DP, DP, C.POINTER(C.c_longlong)],
+    "pf_serve_step": [P, C.POINTER(I), C.POINTER(I)],
+    "pf_serve_finished": [P, C.POINTER(C.c_longlong), I, C.POINTER(I)],
+    "pf_serve_result": [P, C.c_longlong, DP, DP, DP, DP, DP, DP],
+    "pf_serve_stats": [P, C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(C.c_ulonglong),
+                       C.POINTER(C.c_longlong)],
+    "pf_serve_batch": [P, PP],
     "pf_batch_staged": [P, C.POINTER(I)],
     "pf_ctx_launches": [P, C.POINTER(C.c_ulonglong)],
     "pf_prof_enable": [P, I],

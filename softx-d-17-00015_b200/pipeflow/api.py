@@ -215,6 +215,13 @@ class Pipe:
         self.N, self.H, self.Z, self.Th = N.value, H.value, Z.value, Th.value
         self.K, self.M, self.Mp = cfg.K, cfg.M, cfg.Mp
 
+    def reconfigure(self, cfg: PipeConfig):
+        """New physics for the same shape (pf_ctx_reconfigure): a fresh run
+        reusing this pipe's device memory; call vel_matrices again."""
+        c = cfg_struct(cfg)
+        _check(self.lib.pf_ctx_reconfigure(self.ctx, C.byref(c)))
+        self.cfg = cfg
+
     def close(self):
         if self.ctx and self._owned:
             self.lib.pf_ctx_destroy(self.ctx)
@@ -496,9 +503,10 @@ class Batch:
     CUDA graph per batch timestep, each stage launched once over all pipes
     where the pipes allow it, else one kernel chain per pipe."""
 
-    def __init__(self, cfgs, device: int = -1):
+    def __init__(self, cfgs=(), device: int = -1):
         self.lib = L.load()
-        arr = (L.pf_config * len(cfgs))()
+        cfgs = list(cfgs)
+        arr = (L.pf_config * max(1, len(cfgs)))()
         keep = []
         for i, cfg in enumerate(cfgs):
             c = cfg_struct(cfg)
@@ -513,6 +521,19 @@ class Batch:
             ph = C.c_void_p()
             _check(self.lib.pf_batch_pipe(self.h, i, C.byref(ph)))
             self.pipes.append(Pipe(cfg, _handle=ph))
+
+    def attach(self, pipe: "Pipe"):
+        """Add a pipe the caller owns (it must stay open while attached)."""
+        _check(self.lib.pf_batch_attach(self.h, pipe.ctx))
+        self.pipes.append(pipe)
+
+    def detach(self, pipe: "Pipe"):
+        _check(self.lib.pf_batch_detach(self.h, pipe.ctx))
+        self.pipes = [p for p in self.pipes if p is not pipe]
+
+    def set_graphs(self, on: bool):
+        """False: launch every step directly (membership changing every step)."""
+        _check(self.lib.pf_batch_set_graphs(self.h, int(bool(on))))
 
     def matrices(self):
         _check(self.lib.pf_batch_matrices(self.h))
@@ -561,8 +582,81 @@ class Batch:
     def close(self):
         if self.h:
             for p in self.pipes:
-                p.ctx = None
+                if not p._owned:  # the batch's own pipes die with it; attached ones stay open
+                    p.ctx = None
             self.lib.pf_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching request server (pf_serve_*): each request advances
+    a state by nsteps timesteps; admitted requests share one batch."""
+
+    def __init__(self, hbm_budget: int = 150 * 10**9, max_active: int = 4096, orbit: bool = True,
+                 device: int = -1):
+        self.lib = L.load()
+        h = C.c_void_p()
+        self.h = None
+        _check(self.lib.pf_serve_create(device, int(hbm_budget), int(max_active), int(orbit), C.byref(h)))
+        self.h = h
+        self._shape = {}
+
+    def submit(self, cfg: PipeConfig, nsteps: int, state) -> int:
+        """state: (ur, ut, uz), each an (re, im) pair of (N, H) arrays, as
+        Pipe.set_state takes it."""
+        c = cfg_struct(cfg)
+        arrs = []
+        for re, im in state:
+            arrs.append(np.ascontiguousarray(np.asarray(re, dtype=np.float64).T))
+            arrs.append(np.ascontiguousarray(np.asarray(im, dtype=np.float64).T))
+        ptrs = [_dp(a) for a in arrs]
+        rid = C.c_longlong()
+        _check(self.lib.pf_serve_submit(self.h, C.byref(c), int(nsteps), *ptrs, C.byref(rid)))
+        self._shape[rid.value] = (cfg.H, cfg.N)
+        return rid.value
+
+    def step(self):
+        """Admit, advance one timestep, retire; returns (admitted, finished)."""
+        a, f = C.c_int(), C.c_int()
+        _check(self.lib.pf_serve_step(self.h, C.byref(a), C.byref(f)))
+        return a.value, f.value
+
+    def finished(self, cap: int = 4096):
+        ids = (C.c_longlong * cap)()
+        n = C.c_int()
+        _check(self.lib.pf_serve_finished(self.h, ids, cap, C.byref(n)))
+        return [ids[i] for i in range(n.value)]
+
+    def result(self, rid: int):
+        """Final state as Pipe.get_state returns it; the request is forgotten."""
+        H, N = self._shape.pop(rid)
+        out = [np.empty((H, N), dtype=np.float64) for _ in range(6)]
+        _check(self.lib.pf_serve_result(self.h, int(rid), *[_dp(a) for a in out]))
+        a = [np.ascontiguousarray(x.T) for x in out]
+        return [(a[0], a[1]), (a[2], a[3]), (a[4], a[5])]
+
+    def stats(self) -> dict:
+        q, a, p = C.c_int(), C.c_int(), C.c_int()
+        b, s = C.c_ulonglong(), C.c_longlong()
+        _check(self.lib.pf_serve_stats(self.h, C.byref(q), C.byref(a), C.byref(p), C.byref(b), C.byref(s)))
+        return dict(queued=q.value, active=a.value, pooled=p.value, bytes=b.value, steps=s.value)
+
+    def launches(self) -> int:
+        bh = C.c_void_p()
+        _check(self.lib.pf_serve_batch(self.h, C.byref(bh)))
+        n = C.c_ulonglong()
+        _check(self.lib.pf_batch_launches(bh, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if self.h:
+            self.lib.pf_serve_destroy(self.h)
             self.h = None
 
     def __del__(self):
