@@ -211,6 +211,20 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def rank_seeds(rank: int, pipes: int):
+    """Seeds of one rank's pipes: every replica integrates different states."""
+    return [1000 + rank * pipes + i for i in range(pipes)]
+
+
+def max_over_ranks(dist, torch, values, device):
+    """Element-wise max of per-rank timings (the slowest rank sets the time)."""
+    if dist is None:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def dev_timer(torch, stream):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     return e0, e1
@@ -334,7 +348,7 @@ def run_single(args, torch, P, dist, world, rank, local):
 def run_batched(args, torch, P, dist, world, rank, local):
     """One batch of uneven mixed-precision pipes per rank."""
     cfgs = batched_configs(args.pipes)
-    seeds = [1000 + rank * args.pipes + i for i in range(args.pipes)]
+    seeds = rank_seeds(rank, args.pipes)
     batch = P.Batch([P.PipeConfig(**d, precision=P.PF_PREC_MIXED) for d in cfgs], device=local)
     batch.matrices()
     for p, sd in zip(batch.pipes, seeds):
@@ -492,11 +506,7 @@ def main():
 
     run = run_batched if args.workload == "batched" else run_single
     r = run(args, torch, P, dist, world, rank, local)
-    ms, e2e_ms = r["ms"], r["e2e_ms"]
-    if dist:
-        t = torch.tensor([ms, e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms = max_over_ranks(dist, torch, [r["ms"], r["e2e_ms"]], "cuda")
     value = world * r["count"] * args.steps / (ms / 1e3)
     e2e_value = world * r["count"] * r["ne"] / (e2e_ms / 1e3)
 

@@ -337,3 +337,88 @@ def test_adaptive_dt_parity():
         dts.append(g.tim.dt)
     assert len(set(dts)) > 1  # dt did change
     assert O.rel_l2(state_from_dev(g), o.state()) <= 1e-12
+
+
+def test_device_path_matches_golden_fixtures():
+    """The device timestep against the committed oracle fixtures
+    (tests/golden/oracle_small.json, made by tests/golden/make_golden.py)."""
+    import json
+    from pathlib import Path
+    gold = json.loads((Path(__file__).parent / "golden" / "oracle_small.json").read_text())
+    for case in gold["cases"]:
+        o = oracle_pipe(case["cfg"])
+        st = O.seeded_state(o, case["seed"], case["energy"])
+        g = device_pipe(case["cfg"])
+        g.vel_matrices()
+        state_to_dev(g, st)
+        ncorr = [g.timestep() for _ in range(case["steps"])]
+        assert ncorr == case["ncorr"]
+        assert abs(g.energy() - case["energy_after"]) <= 1e-12 * case["energy_after"]
+        (urr, uri), (utr, uti), (uzr, uzi) = g.get_state()
+        for name, (re, im) in (("ur", (urr, uri)), ("ut", (utr, uti)), ("uz", (uzr, uzi))):
+            cs = case["checksums"][name]
+            assert abs(float(np.sum(re)) - cs[0]) <= 1e-10 * max(1.0, abs(cs[0]))
+            assert abs(float(np.sum(im)) - cs[1]) <= 1e-10 * max(1.0, abs(cs[1]))
+        prof = np.array(case["uz_mean_profile"])
+        assert np.max(np.abs(uzr[:, 0] - prof)) <= 1e-12 * np.max(np.abs(prof))
+        K = case["cfg"]["K"]
+        nh11 = (2 * K - 1) + (K - 1) + 1
+        m11 = np.array(case["ur_mode11"])
+        assert np.max(np.abs(urr[:, nh11] - m11[:, 0])) <= 1e-10 * np.max(np.abs(m11))
+        assert np.max(np.abs(uri[:, nh11] - m11[:, 1])) <= 1e-10 * np.max(np.abs(m11))
+
+
+def test_linear_decay_rate_matches_oracle_eigenvalue():
+    """A 1e-8 perturbation of one (k, m) mode, stepped on the device, decays
+    at the rate of the leading eigenvalue of the oracle's linearised one-step
+    map (dense, 6N x 6N, built column by column from oracle steps)."""
+    import math
+    cfgd = dict(N=16, K=2, M=2, Re=500.0, alpha=1.0, dt=0.01)
+    o = oracle_pipe(cfgd)
+    o.vel_matrices()
+    nh, N = 4, o.N  # (k=1, m=1) in the H=5 ordering (0,0),(1,0),(-1,1),(0,1),(1,1)
+    eps = 1e-8
+
+    def pack(st):
+        out = np.empty(6 * N)
+        for c, f in enumerate(st):
+            out[c * 2 * N: c * 2 * N + N] = f.re[:, nh]
+            out[c * 2 * N + N: (c + 1) * 2 * N] = f.im[:, nh]
+        return out
+
+    def unpack(vec):
+        st = [O.Coll.zeros(N, o.H) for _ in range(3)]
+        for c in range(3):
+            st[c].re[:, nh] = vec[c * 2 * N: c * 2 * N + N]
+            st[c].im[:, nh] = vec[c * 2 * N + N: (c + 1) * 2 * N]
+        return st
+
+    def oracle_step(vec):
+        o.set_state(*unpack(vec))
+        o.timestep(orbit=True)
+        return pack(o.state())
+
+    n = 6 * N
+    J = np.empty((n, n))
+    for i in range(n):
+        e = np.zeros(n)
+        e[i] = eps
+        J[:, i] = oracle_step(e) / eps
+    w, V = np.linalg.eig(J)
+    lead = np.argmax(np.abs(w))
+    rate = math.log(abs(w[lead])) / cfgd["dt"]
+    vec = V[:, lead] / np.linalg.norm(V[:, lead])
+    g = device_pipe(cfgd)
+    g.vel_matrices()
+    norms = []
+    for part in (np.real(vec), np.imag(vec)):
+        state_to_dev(g, unpack(eps * part))
+        n0 = np.linalg.norm(eps * part)
+        g.steporbit(20)
+        st = state_from_dev(g)
+        norms.append((n0, np.linalg.norm(pack(st))))
+    n0 = math.sqrt(sum(a * a for a, _ in norms))
+    n1 = math.sqrt(sum(b * b for _, b in norms))
+    measured = math.log(n1 / n0) / (20 * cfgd["dt"])
+    assert rate < 0
+    assert abs(measured - rate) < 1e-3 * abs(rate) + 1e-6

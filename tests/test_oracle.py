@@ -217,3 +217,5 @@ def test_golden_fixtures_match_oracle():
             cs = case["checksums"][name]
             assert abs(float(np.sum(f.re)) - cs[0]) <= 1e-10 * max(1.0, abs(cs[0]))
             assert abs(float(np.sum(f.im)) - cs[1]) <= 1e-10 * max(1.0, abs(cs[1]))
+        prof = np.array(case["uz_mean_profile"])
+        assert np.max(np.abs(uz.re[:, 0] - prof)) <= 1e-12 * np.max(np.abs(prof))
