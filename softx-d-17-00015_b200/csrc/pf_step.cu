@@ -1,5 +1,5 @@
 // Fused vel_step (velocity.f90:367-394) in five launches:
-//   S1 k_step_rhs  : tile of 32 modes x all radial points: optional
+//   S1 k_step_rhs  : tile of 16 modes x all radial points: optional
 //                    nlincorr (timestep.f90:174-184) or N_ := N copy,
 //                    rhs = Lt u_ + N in the u+-/uz variables (velocity.f90:369-373,
 //                    tim_meshmult with the per-mode band rebuilt in registers),
@@ -54,40 +54,68 @@ __device__ __forceinline__ double lap_diag(const DevMesh &dm, const Geo &g, int 
 }
 
 // ------------------------------------------------------------------- S1
-__device__ __forceinline__ void step_rhs_body(const StepArgs &a, int bx) {
-    extern __shared__ double2 rsm[];  // [N][TM]: radial component of pm2rt(rhs)
+// Block = 16 modes x 16 radial row groups; each thread owns RPT rows
+// n = ty + 16 r (RPT = 4 for N <= 64, 8 for N <= 128), so the values it
+// keeps between the two phases stay in registers.  Pointers are held as
+// __restrict__ locals so loads of later rows can be issued before the stores
+// of earlier ones.
+static constexpr int HM = 16;  // modes per S1 block
+static constexpr int HR = 16;  // row groups per S1 block
+
+template <int RPT>
+__device__ __forceinline__ void step_rhs_body(const StepArgs &a, int hb) {
+    extern __shared__ double2 rsm[];  // [N][HM]: radial component of pm2rt(rhs)
     const Geo &g = a.g;
-    const int N = g.N, Hp = g.Hp;
-    const int tx = threadIdx.x % TM, ty = threadIdx.x / TM;
-    const int nh = bx * TM + tx;
+    const int N = g.N;
+    const size_t Hp = g.Hp;
+    const int tx = threadIdx.x % HM, ty = threadIdx.x / HM;
+    const int nh = hb * HM + tx;
     // the corrector's error max (timestep.f90:190-207) restarts here; S5
     // accumulates it after every block of this launch has finished
-    if (a.mode == 1 && bx == 0 && threadIdx.x == 0) a.sc->dterr2_bits = 0ull;
+    if (a.mode == 1 && hb == 0 && threadIdx.x == 0) a.sc->dterr2_bits = 0ull;
     const bool live = nh < g.H;
+    const int nhc = live ? nh : 0;
     int k = 0, m = 0;
     if (live) mode_km(nh, g.K, k, m);
     const double c1 = a.c1, c2 = a.c2;
-    constexpr int RMAX = 16;  // rows per thread (N <= TR*RMAX)
-    double2 tkeep[RMAX], zkeep[RMAX];
-    int rr = 0;
-    for (int n = ty; n < N; n += TR, ++rr) {
+    const double2 *__restrict__ ur_ = a.u_[0] + nhc;
+    const double2 *__restrict__ ut_ = a.u_[1] + nhc;
+    const double2 *__restrict__ uz_ = a.u_[2] + nhc;
+    double2 *__restrict__ N0 = a.Nl[0] + nhc;
+    double2 *__restrict__ N1 = a.Nl[1] + nhc;
+    double2 *__restrict__ N2 = a.Nl[2] + nhc;
+    double2 *__restrict__ P0 = a.N_[0] + nhc;
+    double2 *__restrict__ P1 = a.N_[1] + nhc;
+    double2 *__restrict__ P2 = a.N_[2] + nhc;
+    double2 *__restrict__ v0 = a.v[0] + nhc;
+    double2 *__restrict__ v1 = a.v[1] + nhc;
+    double2 *__restrict__ v2 = a.v[2] + nhc;
+    double2 *__restrict__ prhs = a.prhs + nhc;
+    const double *__restrict__ radLap = a.dm.radLap;
+    const double *__restrict__ drb = a.dm.dr;
+    const double *__restrict__ rp = a.dm.rp;
+    double2 tkeep[RPT], zkeep[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int n = ty + HR * r;
         double2 vp = make_double2(0, 0), vm = vp, vz = vp;
-        if (live) {
-            const size_t at = (size_t)n * Hp + nh;
-            double2 Nr = a.Nl[0][at], Nt = a.Nl[1][at], Nz = a.Nl[2][at];
+        if (live && n < N) {
+            const size_t at = (size_t)n * Hp;
+            // read once (and in the corrector overwritten): stream past L1
+            double2 Nr = __ldcs(N0 + at), Nt = __ldcs(N1 + at), Nz = __ldcs(N2 + at);
             if (a.mode == 1) {  // N = c N + (1-c) N_
                 const double d1 = a.implicit, d2 = 1.0 - a.implicit;
-                const double2 Pr = a.N_[0][at], Pt = a.N_[1][at], Pz = a.N_[2][at];
+                const double2 Pr = __ldcs(P0 + at), Pt = __ldcs(P1 + at), Pz = __ldcs(P2 + at);
                 Nr = make_double2(d1 * Nr.x + d2 * Pr.x, d1 * Nr.y + d2 * Pr.y);
                 Nt = make_double2(d1 * Nt.x + d2 * Pt.x, d1 * Nt.y + d2 * Pt.y);
                 Nz = make_double2(d1 * Nz.x + d2 * Pz.x, d1 * Nz.y + d2 * Pz.y);
-                a.Nl[0][at] = Nr;
-                a.Nl[1][at] = Nt;
-                a.Nl[2][at] = Nz;
+                N0[at] = Nr;
+                N1[at] = Nt;
+                N2[at] = Nz;
             } else {  // N_ := N
-                a.N_[0][at] = Nr;
-                a.N_[1][at] = Nt;
-                a.N_[2][at] = Nz;
+                P0[at] = Nr;
+                P1[at] = Nt;
+                P2[at] = Nz;
             }
             // rhs = Lt u_ + N, accumulated from N in increasing column order
             vp = make_double2(Nr.x - Nt.y, Nr.y + Nt.x);
@@ -95,53 +123,55 @@ __device__ __forceinline__ void step_rhs_body(const StepArgs &a, int bx) {
             vz = Nz;
             const int lo = max(0, n - KL), hi = min(N - 1, n + KL);
             for (int j = lo; j <= hi; ++j) {
-                const size_t aj = (size_t)j * Hp + nh;
-                const double2 r = a.u_[0][aj], t = a.u_[1][aj], z = a.u_[2][aj];
-                const double off = c2 * a.dm.radLap[(KL + n - j) * N + j];
+                const size_t aj = (size_t)j * Hp;
+                const double2 rr = ur_[aj], t = ut_[aj], z = uz_[aj];
+                const double off = c2 * radLap[(KL + n - j) * N + j];
                 double wp = off, wm = off, wz = off;
                 if (j == n) {
                     wp = (off + c2 * lap_diag(a.dm, g, 1, j, k, m)) + c1;
                     wm = (off + c2 * lap_diag(a.dm, g, -1, j, k, m)) + c1;
                     wz = (off + c2 * lap_diag(a.dm, g, 0, j, k, m)) + c1;
                 }
-                vp.x = fma(wp, r.x - t.y, vp.x);
-                vp.y = fma(wp, r.y + t.x, vp.y);
-                vm.x = fma(wm, r.x + t.y, vm.x);
-                vm.y = fma(wm, r.y - t.x, vm.y);
+                vp.x = fma(wp, rr.x - t.y, vp.x);
+                vp.y = fma(wp, rr.y + t.x, vp.y);
+                vm.x = fma(wm, rr.x + t.y, vm.x);
+                vm.y = fma(wm, rr.y - t.x, vm.y);
                 vz.x = fma(wz, z.x, vz.x);
                 vz.y = fma(wz, z.y, vz.y);
             }
-            a.v[0][at] = vp;
-            a.v[1][at] = vm;
-            a.v[2][at] = vz;
+            v0[at] = vp;
+            v1[at] = vm;
+            v2[at] = vz;
         }
         // pm2rt (velocity.f90:98-114)
-        rsm[n * TM + tx] = make_double2(0.5 * (vp.x + vm.x), 0.5 * (vp.y + vm.y));
-        tkeep[rr] = make_double2(0.5 * (vp.y - vm.y), -0.5 * (vp.x - vm.x));
-        zkeep[rr] = vz;
+        if (n < N) rsm[n * HM + tx] = make_double2(0.5 * (vp.x + vm.x), 0.5 * (vp.y + vm.y));
+        tkeep[r] = make_double2(0.5 * (vp.y - vm.y), -0.5 * (vp.x - vm.x));
+        zkeep[r] = vz;
     }
     __syncthreads();
     if (!live) return;
     const double kal = g.alpha * k;
-    rr = 0;
-    for (int n = ty; n < N; n += TR, ++rr) {
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int n = ty + HR * r;
+        if (n >= N) break;
         double2 dv = make_double2(0, 0);
         if (n != 0 && n != N - 1) {  // tim_zerobc
-            const double rm1 = a.dm.rp[2 * N + n];
+            const double rm1 = rp[2 * N + n];
             const double m1r1 = rm1 * g.Mp * m;
             double2 dr = make_double2(0, 0);
             const int lo = max(0, n - KL), hi = min(N - 1, n + KL);
             for (int j = lo; j <= hi; ++j) {
-                const double w = a.dm.dr[(KL + n - j) * N + j];
-                const double2 x = rsm[j * TM + tx];
+                const double w = drb[(KL + n - j) * N + j];
+                const double2 x = rsm[j * HM + tx];
                 dr.x = fma(w, x.x, dr.x);
                 dr.y = fma(w, x.y, dr.y);
             }
-            const double2 r = rsm[n * TM + tx], t = tkeep[rr], z = zkeep[rr];
-            dv.x = r.x * rm1 + dr.x - t.y * m1r1 - z.y * kal;   // variables.f90:472-477
-            dv.y = r.y * rm1 + dr.y + t.x * m1r1 + z.x * kal;
+            const double2 rr = rsm[n * HM + tx], t = tkeep[r], z = zkeep[r];
+            dv.x = rr.x * rm1 + dr.x - t.y * m1r1 - z.y * kal;  // variables.f90:472-477
+            dv.y = rr.y * rm1 + dr.y + t.x * m1r1 + z.x * kal;
         }
-        a.prhs[(size_t)n * Hp + nh] = dv;
+        prhs[(size_t)n * Hp] = dv;
     }
 }
 
@@ -222,7 +252,8 @@ __device__ __forceinline__ void solve_async(const double *__restrict__ lu, const
     }
     cp_async_wait<0>();
     // back substitution; y (this thread's forward output) is read through a
-    // four-deep register queue
+    // four-deep register queue, with streaming loads: each value is read once
+    // and then overwritten by the solution
     auto issue_bwd = [&](int t) {  // step t handles column N-1-t
         const int j = N - 1 - t;
         if (j >= 0) {
@@ -236,13 +267,13 @@ __device__ __forceinline__ void solve_async(const double *__restrict__ lu, const
     for (int t = 0; t < RING; ++t) issue_bwd(t);
     double v[KU + 1];
 #pragma unroll
-    for (int i = 0; i <= KU; ++i) v[i] = (N - 1 - i >= 0) ? out[(size_t)(N - 1 - i) * os] : 0.0;
+    for (int i = 0; i <= KU; ++i) v[i] = (N - 1 - i >= 0) ? __ldcs(out + (size_t)(N - 1 - i) * os) : 0.0;
     constexpr int QY = 4;
     double yq[QY];
 #pragma unroll
     for (int q = 0; q < QY; ++q) {
         const int r = N - 1 - KU - 1 - q;
-        yq[q] = (r >= 0) ? out[(size_t)r * os] : 0.0;
+        yq[q] = (r >= 0) ? __ldcs(out + (size_t)r * os) : 0.0;
     }
     for (int t = 0; t < N; ++t) {
         const int j = N - 1 - t;
@@ -253,7 +284,7 @@ __device__ __forceinline__ void solve_async(const double *__restrict__ lu, const
         for (int q = 0; q < QY - 1; ++q) yq[q] = yq[q + 1];
         {
             const int r = j - KU - 1 - QY;
-            yq[QY - 1] = (r >= 0) ? out[(size_t)r * os] : 0.0;
+            yq[QY - 1] = (r >= 0) ? __ldcs(out + (size_t)r * os) : 0.0;
         }
         double x = v[0];
         if (x != 0.0) {
@@ -292,36 +323,62 @@ __device__ __forceinline__ void solve_pnp_body(const StepArgs &a, int bx) {
 }
 
 // S3: rhs - rt2pm(grad p) (velocity.f90:232-236) with zero boundary rows
-// (velocity.f90:376-378), one thread per (n, mode)
+// (velocity.f90:376-378), one thread per (mode, PR consecutive rows)
+static constexpr int PR = 4;  // S3 rows per thread
+
 __device__ __forceinline__ void step_proj_body(const StepArgs &a, int bx, int by) {
     const Geo &g = a.g;
-    const int nh = bx * blockDim.x + threadIdx.x, n = by;
+    const int nh = bx * blockDim.x + threadIdx.x, n0 = by * PR;
+    const int N = g.N;
     if (nh >= g.H) return;
-    const size_t at = (size_t)n * g.Hp + nh;
-    if (n == 0 || n == g.N - 1) {
-        a.rl[0][at] = a.rl[1][at] = a.rl[2][at] = make_double2(0.0, 0.0);
-        return;
-    }
+    const size_t Hp = g.Hp;
+    const double2 *__restrict__ p = a.p + nh;
+    const double2 *__restrict__ v0 = a.v[0] + nh;
+    const double2 *__restrict__ v1 = a.v[1] + nh;
+    const double2 *__restrict__ v2 = a.v[2] + nh;
+    double2 *__restrict__ r0 = a.rl[0] + nh;
+    double2 *__restrict__ r1 = a.rl[1] + nh;
+    double2 *__restrict__ r2 = a.rl[2] + nh;
+    const double *__restrict__ drb = a.dm.dr;
     int k, m;
     mode_km(nh, g.K, k, m);
-    const int N = g.N;
-    double2 dr2 = make_double2(0, 0);
-    const int lo = max(0, n - KL), hi = min(N - 1, n + KL);
-    for (int j = lo; j <= hi; ++j) {
-        const double w = a.dm.dr[(KL + n - j) * N + j];
-        const double2 x = a.p[(size_t)j * g.Hp + nh];
-        dr2.x = fma(w, x.x, dr2.x);
-        dr2.y = fma(w, x.y, dr2.y);
-    }
-    const double2 pv = a.p[at];
-    const double m1r1 = a.dm.rp[2 * N + n] * g.Mp * m;
     const double kal = g.alpha * k;
-    // grad p = (dr p, i m/r p, i alpha k p); rt2pm of its (r, theta) parts
-    const double tRe = -pv.y * m1r1, tIm = pv.x * m1r1;
-    const double2 vp = a.v[0][at], vm = a.v[1][at], vz = a.v[2][at];
-    a.rl[0][at] = make_double2(vp.x - (dr2.x - tIm), vp.y - (dr2.y + tRe));
-    a.rl[1][at] = make_double2(vm.x - (dr2.x + tIm), vm.y - (dr2.y - tRe));
-    a.rl[2][at] = make_double2(vz.x - (-pv.y * kal), vz.y - (pv.x * kal));
+    // the pressure rows this thread's band products touch, loaded once
+    double2 pw[PR + 2 * KL];
+#pragma unroll
+    for (int i = 0; i < PR + 2 * KL; ++i) {
+        const int j = n0 - KL + i;
+        pw[i] = (j >= 0 && j < N) ? p[(size_t)j * Hp] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int q = 0; q < PR; ++q) {
+        const int n = n0 + q;
+        if (n >= N) break;
+        const size_t at = (size_t)n * Hp;
+        if (n == 0 || n == N - 1) {
+            r0[at] = r1[at] = r2[at] = make_double2(0.0, 0.0);
+            continue;
+        }
+        double2 dr2 = make_double2(0, 0);
+        const int lo = max(0, n - KL), hi = min(N - 1, n + KL);
+#pragma unroll
+        for (int d = -KL; d <= KL; ++d) {
+            const int j = n + d;
+            if (j < lo || j > hi) continue;
+            const double w = drb[(KL + n - j) * N + j];
+            const double2 x = pw[q + KL + d];
+            dr2.x = fma(w, x.x, dr2.x);
+            dr2.y = fma(w, x.y, dr2.y);
+        }
+        const double2 pv = pw[q + KL];
+        const double m1r1 = a.dm.rp[2 * N + n] * g.Mp * m;
+        // grad p = (dr p, i m/r p, i alpha k p); rt2pm of its (r, theta) parts
+        const double tRe = -pv.y * m1r1, tIm = pv.x * m1r1;
+        const double2 vp = v0[at], vm = v1[at], vz = v2[at];
+        r0[at] = make_double2(vp.x - (dr2.x - tIm), vp.y - (dr2.y + tRe));
+        r1[at] = make_double2(vm.x - (dr2.x + tIm), vm.y - (dr2.y - tRe));
+        r2[at] = make_double2(vz.x - (-pv.y * kal), vz.y - (pv.x * kal));
+    }
 }
 
 // S4: warp = one (system, re/im) of 32 consecutive modes; the pivot-free
@@ -398,38 +455,72 @@ __device__ __forceinline__ void step_final_body(const StepArgs &a, int bx) {
     double err = 0.0;
     if (live) {
         const double *cf = coef[tx];
-        for (int n = ty; n < N; n += TR) {
-            const size_t at = (size_t)n * Hp + nh;
-            double2 r = a.v[0][at], t = a.v[1][at], z = a.v[2][at];
-            if (nh != 0) {
-                const double U1 = a.U[(size_t)(0 * N + n) * Hp + nh], U2 = a.U[(size_t)(1 * N + n) * Hp + nh];
-                const double U3 = a.U[(size_t)(2 * N + n) * Hp + nh], U4 = a.U[(size_t)(3 * N + n) * Hp + nh];
-                const double U5 = a.U[(size_t)(4 * N + n) * Hp + nh], U6 = a.U[(size_t)(5 * N + n) * Hp + nh];
-                r.x = r.x + cf[0] * U1; r.y = r.y + cf[4] * U1;
-                t.x = t.x + cf[1] * U2; t.y = t.y + cf[5] * U2;
-                z.x = z.x - cf[6] * U3; z.y = z.y + cf[2] * U3;
-                r.x = r.x + cf[3] * U4; r.y = r.y + cf[7] * U4;
-                t.x = t.x + cf[3] * U5; t.y = t.y + cf[7] * U5;
-                z.x = z.x - cf[7] * U6; z.y = z.y + cf[3] * U6;
+        const double2 *__restrict__ v0 = a.v[0] + nh;
+        const double2 *__restrict__ v1 = a.v[1] + nh;
+        const double2 *__restrict__ v2 = a.v[2] + nh;
+        const double *__restrict__ Uc = a.U + nh;
+        double2 *__restrict__ u0 = a.u[0] + nh;
+        double2 *__restrict__ u1 = a.u[1] + nh;
+        double2 *__restrict__ u2 = a.u[2] + nh;
+        const size_t NH = (size_t)N * Hp;
+        // rows are taken two at a time and every load of both rows is issued
+        // before either row's stores, so two rows' memory latencies overlap
+        constexpr int RB = 2;
+        for (int n0 = ty; n0 < N; n0 += RB * TR) {
+            double2 r[RB], t[RB], z[RB], o[RB][3];
+            double Uv[RB][6];
+#pragma unroll
+            for (int q = 0; q < RB; ++q) {
+                const int n = n0 + q * TR;
+                if (n >= N) break;
+                const size_t at = (size_t)n * Hp;
+                r[q] = v0[at];
+                t[q] = v1[at];
+                z[q] = v2[at];
+                if (nh != 0) {
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) Uv[q][i] = Uc[i * NH + at];
+                }
+                if (a.mode == 1 && nh != 0) {  // read once, overwritten below: stream past L1
+                    o[q][0] = __ldcs(u0 + at);
+                    o[q][1] = __ldcs(u1 + at);
+                    o[q][2] = __ldcs(u2 + at);
+                }
             }
-            // pm2rt
-            const double2 ur = make_double2(0.5 * (r.x + t.x), 0.5 * (r.y + t.y));
-            const double2 ut = make_double2(0.5 * (r.y - t.y), -0.5 * (r.x - t.x));
-            if (nh == 0) {
-                m0buf[0][0][n] = ur.x; m0buf[0][1][n] = ur.y;
-                m0buf[1][0][n] = ut.x; m0buf[1][1][n] = ut.y;
-                m0buf[2][0][n] = z.x;  m0buf[2][1][n] = z.y;
-                continue;
+#pragma unroll
+            for (int q = 0; q < RB; ++q) {
+                const int n = n0 + q * TR;
+                if (n >= N) break;
+                const size_t at = (size_t)n * Hp;
+                double2 rr = r[q], tt = t[q], zz = z[q];
+                if (nh != 0) {
+                    const double U1 = Uv[q][0], U2 = Uv[q][1], U3 = Uv[q][2];
+                    const double U4 = Uv[q][3], U5 = Uv[q][4], U6 = Uv[q][5];
+                    rr.x = rr.x + cf[0] * U1; rr.y = rr.y + cf[4] * U1;
+                    tt.x = tt.x + cf[1] * U2; tt.y = tt.y + cf[5] * U2;
+                    zz.x = zz.x - cf[6] * U3; zz.y = zz.y + cf[2] * U3;
+                    rr.x = rr.x + cf[3] * U4; rr.y = rr.y + cf[7] * U4;
+                    tt.x = tt.x + cf[3] * U5; tt.y = tt.y + cf[7] * U5;
+                    zz.x = zz.x - cf[7] * U6; zz.y = zz.y + cf[3] * U6;
+                }
+                // pm2rt
+                const double2 ur = make_double2(0.5 * (rr.x + tt.x), 0.5 * (rr.y + tt.y));
+                const double2 ut = make_double2(0.5 * (rr.y - tt.y), -0.5 * (rr.x - tt.x));
+                if (nh == 0) {
+                    m0buf[0][0][n] = ur.x; m0buf[0][1][n] = ur.y;
+                    m0buf[1][0][n] = ut.x; m0buf[1][1][n] = ut.y;
+                    m0buf[2][0][n] = zz.x; m0buf[2][1][n] = zz.y;
+                    continue;
+                }
+                if (a.mode == 1) {
+                    err = fmax(err, sq(make_double2(o[q][0].x - ur.x, o[q][0].y - ur.y)));
+                    err = fmax(err, sq(make_double2(o[q][1].x - ut.x, o[q][1].y - ut.y)));
+                    err = fmax(err, sq(make_double2(o[q][2].x - zz.x, o[q][2].y - zz.y)));
+                }
+                u0[at] = ur;
+                u1[at] = ut;
+                u2[at] = zz;
             }
-            if (a.mode == 1) {
-                const double2 o0 = a.u[0][at], o1 = a.u[1][at], o2 = a.u[2][at];
-                err = fmax(err, sq(make_double2(o0.x - ur.x, o0.y - ur.y)));
-                err = fmax(err, sq(make_double2(o1.x - ut.x, o1.y - ut.y)));
-                err = fmax(err, sq(make_double2(o2.x - z.x, o2.y - z.y)));
-            }
-            a.u[0][at] = ur;
-            a.u[1][at] = ut;
-            a.u[2][at] = z;
         }
     }
     if (bx == 0) {  // mode 0: flux adjustment and symmetry zeros
@@ -465,17 +556,24 @@ __device__ __forceinline__ void step_final_body(const StepArgs &a, int bx) {
         }
         if (threadIdx.x == 0 && a.const_flux) a.sc->Pr0 = a.sc->Pr0 + d3 * g.Re / 4.0;
     }
-    if (a.mode == 1) {
+    if (a.mode == 1) {  // one atomic per block: warp maxima, then the block's
+        __shared__ double wmax[TM * TR / 32];
         for (int o = 16; o > 0; o >>= 1) err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
-        if ((threadIdx.x & 31) == 0)
-            atomicMax(&a.sc->dterr2_bits, (unsigned long long)__double_as_longlong(err));
+        if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = err;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double e = wmax[0];
+            for (int i = 1; i < TM * TR / 32; ++i) e = fmax(e, wmax[i]);
+            atomicMax(&a.sc->dterr2_bits, (unsigned long long)__double_as_longlong(e));
+        }
     }
 }
 
 // ------------------------------------------------------------- kernels
 // Lone pipe: one launch per stage over that pipe's tiles.  Batch: one launch
 // per stage over the tiles of every pipe, blk[b] = (pipe, tile of that pipe).
-__global__ void __launch_bounds__(TM *TR) k_step_rhs(StepArgs a) { step_rhs_body(a, blockIdx.x); }
+template <int RPT>
+__global__ void __launch_bounds__(HM *HR, 3) k_step_rhs(StepArgs a) { step_rhs_body<RPT>(a, blockIdx.x); }
 __global__ void __launch_bounds__(64) k_solve_pnp(StepArgs a) { solve_pnp_body(a, blockIdx.x); }
 __global__ void k_step_proj(StepArgs a) { step_proj_body(a, blockIdx.x, blockIdx.y); }
 __global__ void __launch_bounds__(192) k_solve_ld(StepArgs a) { solve_ld_body(a, blockIdx.x); }
@@ -487,11 +585,18 @@ __global__ void __launch_bounds__(TM *TR) k_step_final(StepArgs a) { step_final_
         const StepArgs a = args[pb.x]; /* by value: stores cannot alias it */                  \
         BODY(a, pb.y);                                                                         \
     }
-PF_BATCH1(k_step_rhs_batch, step_rhs_body, __launch_bounds__(TM *TR))
 PF_BATCH1(k_solve_pnp_batch, solve_pnp_body, __launch_bounds__(64))
 PF_BATCH1(k_solve_ld_batch, solve_ld_body, __launch_bounds__(192))
 PF_BATCH1(k_step_final_batch, step_final_body, __launch_bounds__(TM *TR))
 #undef PF_BATCH1
+
+template <int RPT>
+__global__ void __launch_bounds__(HM *HR, 3) k_step_rhs_batch(const StepArgs *__restrict__ args,
+                                                             const int2 *__restrict__ blk) {
+    const int2 pb = blk[blockIdx.x];
+    const StepArgs a = args[pb.x];  // by value: stores cannot alias it
+    step_rhs_body<RPT>(a, pb.y);
+}
 
 __global__ void __launch_bounds__(128) k_step_proj_batch(const StepArgs *__restrict__ args, const int2 *__restrict__ blk) {
     const int2 pb = blk[blockIdx.x];
@@ -543,6 +648,8 @@ static bool any_ld_pivoted(const pf_ctx *ctx) {
     return ctx->LDp.pivoted || ctx->LDm.pivoted || ctx->LDz.pivoted;
 }
 
+static size_t rhs_smem(int N) { return (size_t)N * HM * sizeof(double2); }
+
 static int step_attrs() {
     static bool attrs_set = false;
     if (!attrs_set) {
@@ -552,12 +659,17 @@ static int step_attrs() {
         PF_CUDA(cudaFuncSetAttribute(k_solve_pnp, cudaFuncAttributeMaxDynamicSharedMemorySize, pnp));
         PF_CUDA(cudaFuncSetAttribute(k_solve_ld_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, ld));
         PF_CUDA(cudaFuncSetAttribute(k_solve_pnp_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, pnp));
+        const int rhs = (int)rhs_smem(128);
+        PF_CUDA(cudaFuncSetAttribute(k_step_rhs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, rhs));
+        PF_CUDA(cudaFuncSetAttribute(k_step_rhs<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, rhs));
+        PF_CUDA(cudaFuncSetAttribute(k_step_rhs_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, rhs));
+        PF_CUDA(cudaFuncSetAttribute(k_step_rhs_batch<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, rhs));
         attrs_set = true;
     }
     return PF_OK;
 }
 
-static bool pf_fused_step_geo_ok(const Geo &g) { return g.N <= TR * 16 && g.N <= 128; }
+static bool pf_fused_step_geo_ok(const Geo &g) { return g.N <= HR * 8; }
 
 // One predictor (corrector=0) or corrector (corrector=1) vel_step.  The
 // predictor's u_ := u copy is a pointer swap of vel[0..2] and prev[0..2].
@@ -577,7 +689,10 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
     PF_TRY(step_attrs());
     {
         ProfScope ps_(ctx, PF_K_STEP);
-        k_step_rhs<<<tiles, TM * TR, (size_t)g.N * TM * sizeof(double2), ctx->stream>>>(a);
+        if (g.N <= HR * 4)
+            k_step_rhs<4><<<grid1(g.H, HM), HM * HR, rhs_smem(g.N), ctx->stream>>>(a);
+        else
+            k_step_rhs<8><<<grid1(g.H, HM), HM * HR, rhs_smem(g.N), ctx->stream>>>(a);
     }
     PF_LAUNCHED(ctx);
     {
@@ -587,7 +702,7 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
     PF_LAUNCHED(ctx);
     {
         ProfScope ps_(ctx, PF_K_STEP);
-        k_step_proj<<<dim3(grid1(g.H, 128), g.N), 128, 0, ctx->stream>>>(a);
+        k_step_proj<<<dim3(grid1(g.H, 128), grid1(g.N, PR)), 128, 0, ctx->stream>>>(a);
     }
     PF_LAUNCHED(ctx);
     {
@@ -609,8 +724,8 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
 struct pf_step_batch {
     int n;
     StepArgs *d_args[2][2];  // [pointer state after the predictor's swap][mode]
-    int2 *tile, *proj;       // (pipe, tile) maps: 32-mode tiles, 128-mode x row tiles
-    int ntile, nproj;
+    int2 *tile, *proj, *half;  // (pipe, tile) maps: 32-mode tiles, 128-mode x row tiles, 16-mode tiles
+    int ntile, nproj, nhalf;
     int maxN;
     bool anypiv;
 };
@@ -620,6 +735,7 @@ void pf_step_batch_free(pf_step_batch *b) {
     for (int s = 0; s < 2; ++s)
         for (int m = 0; m < 2; ++m) cudaFree(b->d_args[s][m]);
     cudaFree(b->tile);
+    cudaFree(b->half);
     cudaFree(b->proj);
     delete b;
 }
@@ -632,7 +748,7 @@ int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
     b->maxN = 0;
     b->anypiv = false;
     std::vector<StepArgs> h(n);
-    std::vector<int2> tile, proj;
+    std::vector<int2> tile, proj, half;
     for (int i = 0; i < n; ++i) {
         const Geo &g = pipes[i]->g;
         if (!pf_fused_step_geo_ok(g)) {
@@ -643,7 +759,8 @@ int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
         b->maxN = std::max(b->maxN, g.N);
         b->anypiv |= any_ld_pivoted(pipes[i]);
         for (int t = 0; t < (int)grid1(g.H, TM); ++t) tile.push_back(make_int2(i, t));
-        for (int t = 0; t < (int)grid1(g.H, 128) * g.N; ++t) proj.push_back(make_int2(i, t));
+        for (int t = 0; t < (int)grid1(g.H, HM); ++t) half.push_back(make_int2(i, t));
+        for (int t = 0; t < (int)(grid1(g.H, 128) * grid1(g.N, PR)); ++t) proj.push_back(make_int2(i, t));
     }
     for (int s = 0; s < 2; ++s)
         for (int m = 0; m < 2; ++m) {
@@ -661,6 +778,13 @@ int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
             }
         }
     b->ntile = (int)tile.size();
+    b->nhalf = (int)half.size();
+    if (cudaMalloc((void **)&b->half, half.size() * sizeof(int2)) != cudaSuccess ||
+        cudaMemcpy(b->half, half.data(), half.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess) {
+        pf_step_batch_free(b);
+        pf_set_error("batched step: tile map upload failed");
+        return PF_ERR_CUDA;
+    }
     b->nproj = (int)proj.size();
     if (cudaMalloc((void **)&b->tile, tile.size() * sizeof(int2)) != cudaSuccess ||
         cudaMalloc((void **)&b->proj, proj.size() * sizeof(int2)) != cudaSuccess ||
@@ -683,7 +807,10 @@ int pf_step_batch_launch(pf_step_batch *b, int state, int corrector, cudaStream_
     const int ldsw = b->anypiv ? KV + 1 : KL + 1;
     {
         StageScope ss_(prof, PF_K_STEP, st);
-        k_step_rhs_batch<<<b->ntile, TM * TR, (size_t)b->maxN * TM * sizeof(double2), st>>>(a, b->tile);
+        if (b->maxN <= HR * 4)
+            k_step_rhs_batch<4><<<b->nhalf, HM * HR, rhs_smem(b->maxN), st>>>(a, b->half);
+        else
+            k_step_rhs_batch<8><<<b->nhalf, HM * HR, rhs_smem(b->maxN), st>>>(a, b->half);
     }
     PF_CHECK_LAUNCH();
     {
