@@ -189,6 +189,7 @@ static int ctx_init(pf_ctx *ctx, const pf_config *cfg, int device) {
     PF_TRY(pf_alloc(ctx, (void **)&ctx->Ui, (size_t)N * sizeof(double)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->red, (size_t)(3 * N + g.Hp + 64) * sizeof(double)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->cflmax, (size_t)3 * N * sizeof(unsigned long long)));
+    PF_TRY(pf_alloc(ctx, (void **)&ctx->mpart, (size_t)((g.H + 31) / 32) * N * 3 * sizeof(double)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->anypiv, sizeof(int)));
     ctx->T_bytes = (size_t)6 * N * g.M * g.Z * sizeof(double2);
     PF_TRY(pf_alloc(ctx, &ctx->T, ctx->T_bytes));

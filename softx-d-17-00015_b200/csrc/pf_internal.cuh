@@ -163,6 +163,7 @@ struct pf_ctx {
     double *Ainv;        // inverted 4x4 [(i*4+j)*Hp + nh] == A(i+1,j+1,nh)
     double *Ui;          // flux influence vector [N]
     double *red;         // reduction scratch (>= 3*N + H doubles)
+    double *mpart;       // FP64 mean-mode partial sums [ceil(H/32)][N][3]
     unsigned long long *cflmax;  // 3*N CFL maxima of the last fused transform
     bool cfl_fused;              // cflmax is current (else use vel_r/t/z)
     int *anypiv;         // per LU set: 1 if dgbtf2 swapped any row
@@ -240,6 +241,17 @@ inline double bits_to_double(unsigned long long b) {
 // of pointers copied into a kernel stays in registers
 template <typename T> __device__ __forceinline__ T pick3(T const (&p)[3], int i) {
     return i == 0 ? p[0] : (i == 1 ? p[1] : p[2]);
+}
+
+// x / d for 0 <= x < 2^22 and d > 0, given inv = 1.0f / d: a float
+// reciprocal estimate corrected by one step (cheaper than a run-time integer
+// division inside index loops)
+__device__ __forceinline__ int fdiv(int x, int d, float inv) {
+    int q = __float2int_rz((float)x * inv);
+    const int r = x - q * d;
+    if (r < 0) --q;
+    else if (r >= d) ++q;
+    return q;
 }
 
 inline unsigned grid1(long long n, int block) {

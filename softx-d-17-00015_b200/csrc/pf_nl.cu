@@ -19,6 +19,7 @@
 #include "pf_fftcore.cuh"
 
 static constexpr int NL_THREADS = 256;
+static constexpr int MEAN_THREADS = 256;  // FP64 mean-mode partial sums (mixed precision)
 
 struct NLArgs {
     const double2 *u[3];
@@ -31,6 +32,7 @@ struct NLArgs {
     void *T;                  // (m, z) intermediate, compute type
     const void *twz, *twt;    // twiddle tables, compute type
     int MC, ZC;               // z-pass columns and theta-pass rows per block
+    double *mpart;            // FP64 mean-mode partial sums [ceil(H/32)][N][3]
 };
 
 template <typename C> __device__ __forceinline__ C to_c(double2 v);
@@ -140,9 +142,10 @@ __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
     __syncthreads();
     // Hermitian-extend the M retained theta modes of two z rows into one
     // complex row: X = a + i b (c2r ignores the DC imaginary parts)
+    const float inp = 1.0f / np, inM = 1.0f / M;
     for (int idx = threadIdx.x; idx < 6 * M * np; idx += blockDim.x) {
-        const int zp = idx % np, rest = idx / np;
-        const int m = rest % M, comp = rest / M;
+        const int rest = fdiv(idx, np, inp), zp = idx - rest * np;
+        const int comp = fdiv(rest, M, inM), m = rest - comp * M;
         const int za = z0 + 2 * zp, zb = za + 1;
         const C *col = T + ((size_t)(comp * g.N + n) * M + m) * Z;
         const C va = (za < Z) ? col[za] : CTraits<C>::make(0, 0);
@@ -182,6 +185,7 @@ __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
         mt = fmax(mt, fmax(fabs(u[1].x), hasb ? fabs(u[1].y) : (R)0));
         mz = fmax(mz, fmax(fabs(u[2].x + base), hasb ? fabs(u[2].y + base) : (R)0));
     }
+    __shared__ double cflw[3][NL_THREADS / 32];  // warp maxima; three atomics per block
     if (a.cfl) {
         for (int o = 16; o > 0; o >>= 1) {
             mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
@@ -189,17 +193,22 @@ __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
             mz = fmax(mz, __shfl_xor_sync(0xffffffffu, mz, o));
         }
         if ((threadIdx.x & 31) == 0) {
-            atomic_max_pos(&a.cfl[3 * n + 0], (double)mr);
-            atomic_max_pos(&a.cfl[3 * n + 1], (double)mt);
-            atomic_max_pos(&a.cfl[3 * n + 2], (double)mz);
+            cflw[0][threadIdx.x >> 5] = (double)mr;
+            cflw[1][threadIdx.x >> 5] = (double)mt;
+            cflw[2][threadIdx.x >> 5] = (double)mz;
         }
     }
     __syncthreads();
+    if (a.cfl && threadIdx.x < 3) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v = fmax(v, cflw[threadIdx.x][w]);
+        atomic_max_pos(&a.cfl[3 * n + threadIdx.x], v);
+    }
     FR::template run<-1>(prod, 3 * np, tw, tw2);
     // separate the two packed real transforms and keep m < M
     for (int idx = threadIdx.x; idx < 3 * M * np; idx += blockDim.x) {
-        const int zp = idx % np, rest = idx / np;
-        const int m = rest % M, comp = rest / M;
+        const int rest = fdiv(idx, np, inp), zp = idx - rest * np;
+        const int comp = fdiv(rest, M, inM), m = rest - comp * M;
         const C *X = prod + (comp * np + zp) * RS;
         const C A = X[m], B = X[(TL - m) % TL];
         const C va = CTraits<C>::make((R)0.5 * (A.x + B.x), (R)0.5 * (A.y - B.y));
@@ -242,8 +251,9 @@ __device__ __forceinline__ void nl_zfwd_body(const NLArgs &a, int bx, int by, in
         if (n == 0 && m0 == 0 && threadIdx.x == 0) a.sc->Pr0 = Pr0;
     }
     double2 *f = pick3(a.N, comp) + (size_t)n * g.Hp;
+    const float ik = 1.0f / (2 * K - 1);
     for (int idx = threadIdx.x; idx < mc * (2 * K - 1); idx += blockDim.x) {
-        const int c = idx / (2 * K - 1), kk = idx - c * (2 * K - 1) - (K - 1);
+        const int c = fdiv(idx, 2 * K - 1, ik), kk = idx - c * (2 * K - 1) - (K - 1);
         const int m = m0 + c;
         if (m == 0 && kk < 0) continue;
         const int nh = m * (2 * K - 1) + kk;
@@ -338,6 +348,7 @@ static NLArgs make_nl_args(pf_ctx *ctx) {
     a.sc = ctx->dsc;
     a.cfl = ctx->cflmax;
     a.T = ctx->T;
+    a.mpart = ctx->mpart;
     const bool mixed = ctx->cfg.precision == PF_PREC_MIXED;
     a.twz = mixed ? (const void *)ctx->twZf : (const void *)ctx->twZ;
     a.twt = mixed ? (const void *)ctx->twTf : (const void *)ctx->twT;
@@ -413,9 +424,12 @@ static int launch_nl(pf_ctx *ctx, const NLArgs &a) {
     return PF_OK;
 }
 
-__global__ void k_nl_mean64(NLArgs a);
+__global__ void k_nl_mean64_part(NLArgs a);
+__global__ void k_nl_mean64_fin(NLArgs a);
+static int mean_attrs();
+static size_t mean_smem(int N);
 
-// vel_transform + vel_nonlinear in three launches (four in mixed precision);
+// vel_transform + vel_nonlinear in three launches (five in mixed precision);
 // CFL maxima per radial point are left in ctx->cflmax.
 int pf_launch_nl_fused(pf_ctx *ctx) {
     const NLArgs a = make_nl_args(ctx);
@@ -423,7 +437,10 @@ int pf_launch_nl_fused(pf_ctx *ctx) {
         PF_TRY(launch_nl<float2>(ctx, a));
         {
             ProfScope ps_(ctx, PF_K_ZFWD);
-            k_nl_mean64<<<ctx->g.N, 256, 0, ctx->stream>>>(a);
+            PF_TRY(mean_attrs());
+            k_nl_mean64_part<<<(ctx->g.H + 31) / 32, MEAN_THREADS, mean_smem(ctx->g.N), ctx->stream>>>(a);
+            PF_LAUNCHED(ctx);
+            k_nl_mean64_fin<<<(ctx->g.N + 3) / 4, 128, 0, ctx->stream>>>(a);
         }
         PF_LAUNCHED(ctx);
         return PF_OK;
@@ -438,50 +455,108 @@ int pf_launch_nl_fused(pf_ctx *ctx) {
 // modes aliases onto (0,0), so the grid mean equals the spectral sum
 //   mean(f g) = Re f00 Re g00 + 2 sum_{k>=1} Re(f_k0 conj g_k0)
 //             + 2 sum_{m>=1, all k} Re(f_km conj g_km)
-// (the c2r transform ignores Im f00).  One block per radial point.
-__device__ __forceinline__ void nl_mean64_body(const NLArgs &a, int n) {
+// (the c2r transform ignores Im f00).  Two launches.  The first: one block
+// per 32-mode chunk, u_t and u_z of those modes at every radial point staged
+// in shared memory (each value read from HBM once), one warp per radial
+// point at a time (lanes = modes), the curl formed from the staged rows and
+// the chunk's sums written as partials.  The second: one warp per radial
+// point adds the chunks' partials in a fixed order.
+__device__ __forceinline__ void nl_mean64_part_body(const NLArgs &a, int chunk) {
+    extern __shared__ double2 msm[];  // [2][N][32]: u_t, u_z of this chunk's modes
     const Geo &g = a.g;
-    double s[3] = {0.0, 0.0, 0.0};
-    for (int nh = threadIdx.x; nh < g.H; nh += blockDim.x) {
-        int k, m;
-        mode_km(nh, g.K, k, m);
-        double2 u[6];
-        for (int c = 0; c < 6; ++c) u[c] = nl_input(a, c, n, nh, k, m);
-        const double w = (nh == 0) ? 1.0 : 2.0;
-        auto dot = [&](double2 f, double2 h) { return nh == 0 ? f.x * h.x : f.x * h.x + f.y * h.y; };
-        s[0] += w * (dot(u[1], u[5]) - dot(u[2], u[4]));
-        s[1] += w * (dot(u[2], u[3]) - dot(u[0], u[5]));
-        s[2] += w * (dot(u[0], u[4]) - dot(u[1], u[3]));
-    }
-    __shared__ double red[3][32];
-    for (int c = 0; c < 3; ++c) {
-        double v = s[c];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((threadIdx.x & 31) == 0) red[c][threadIdx.x >> 5] = v;
+    const int N = g.N, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int nh = chunk * 32 + lane;
+    const bool live = nh < g.H;
+    const size_t Hp = g.Hp;
+    double2 *st = msm, *sz = msm + N * 32;
+    for (int n = warp; n < N; n += nw) {
+        const size_t at = (size_t)n * Hp + nh;
+        st[n * 32 + lane] = live ? a.u[1][at] : make_double2(0.0, 0.0);
+        sz[n * 32 + lane] = live ? a.u[2][at] : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double t[3] = {0.0, 0.0, 0.0};
-        for (int c = 0; c < 3; ++c)
-            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t[c] += red[c][i];
-        const size_t at = (size_t)n * g.Hp;  // nh = 0
-        // vel_addHPF at k=m=0: a = 0; N_z += -U' u_r (u_r(0,0) is zero after
-        // imposesym but kept for fidelity) and the constant-flux pressure
-        const double2 ur = a.u[0][at];
-        double zr = t[2] + (-a.dm.velUp[n]) * ur.x;
-        if (a.const_flux) {
-            double Pr0 = 0.0;
-            for (int j = 0; j <= KL; ++j) Pr0 += a.u[2][(size_t)(g.N - 1 - KL + j) * g.Hp].x * a.dm.dr1[1 * (KL + 1) + j];
-            Pr0 = Pr0 / (-2.0);
-            zr = zr + 4.0 * Pr0 / g.Re;
+    int k = 0, m = 0;
+    if (live) mode_km(nh, g.K, k, m);
+    const double k1a1 = g.alpha * k;
+    const double *__restrict__ drb = a.dm.dr;
+    for (int n = warp; n < N; n += nw) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        if (live) {
+            const double2 ur = a.u[0][(size_t)n * Hp + nh], ut = st[n * 32 + lane], uz = sz[n * 32 + lane];
+            const double rm1 = a.dm.rp[2 * N + n];
+            const double m1r1 = rm1 * g.Mp * m;
+            const int lo = max(0, n - KL), hi = min(N - 1, n + KL);
+            double2 dz = make_double2(0.0, 0.0), dt = dz;
+            for (int j = lo; j <= hi; ++j) {  // d/dr of u_z and u_t (var_coll_meshmult)
+                const double w = drb[(KL + n - j) * N + j];
+                const double2 z = sz[j * 32 + lane], t = st[j * 32 + lane];
+                dz.x = fma(w, z.x, dz.x);
+                dz.y = fma(w, z.y, dz.y);
+                dt.x = fma(w, t.x, dt.x);
+                dt.y = fma(w, t.y, dt.y);
+            }
+            // curl (variables.f90:408-436)
+            const double2 cr = make_double2(-uz.y * m1r1 + ut.y * k1a1, uz.x * m1r1 - ut.x * k1a1);
+            const double2 ct = make_double2(-ur.y * k1a1 - dz.x, ur.x * k1a1 - dz.y);
+            const double2 cz = make_double2(ut.x * rm1 + dt.x + ur.y * m1r1, ut.y * rm1 + dt.y - ur.x * m1r1);
+            const double w = (nh == 0) ? 1.0 : 2.0;
+            auto dot = [&](double2 f, double2 h) { return nh == 0 ? f.x * h.x : f.x * h.x + f.y * h.y; };
+            s0 = w * (dot(ut, cz) - dot(uz, ct));
+            s1 = w * (dot(uz, cr) - dot(ur, cz));
+            s2 = w * (dot(ur, ct) - dot(ut, cr));
         }
-        a.N[0][at] = make_double2(t[0], 0.0);
-        a.N[1][at] = make_double2(t[1], 0.0);
-        a.N[2][at] = make_double2(zr, (-a.dm.velUp[n]) * ur.y);
+        for (int o = 16; o > 0; o >>= 1) {
+            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        }
+        if (lane == 0) {
+            double *dst = a.mpart + ((size_t)chunk * N + n) * 3;
+            dst[0] = s0;
+            dst[1] = s1;
+            dst[2] = s2;
+        }
     }
 }
 
-__global__ void k_nl_mean64(NLArgs a) { nl_mean64_body(a, blockIdx.x); }
+__device__ __forceinline__ void nl_mean64_fin_body(const NLArgs &a, int n) {
+    const Geo &g = a.g;
+    const int lane = threadIdx.x & 31;
+    const int nchunk = (g.H + 31) / 32;
+    double t[3] = {0.0, 0.0, 0.0};
+    for (int c = lane; c < nchunk; c += 32) {
+        const double *src = a.mpart + ((size_t)c * g.N + n) * 3;
+        t[0] += src[0];
+        t[1] += src[1];
+        t[2] += src[2];
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        for (int o = 16; o > 0; o >>= 1) t[q] += __shfl_xor_sync(0xffffffffu, t[q], o);
+    if (lane != 0) return;
+    const size_t at = (size_t)n * g.Hp;  // nh = 0
+    // vel_addHPF at k=m=0: a = 0; N_z += -U' u_r (u_r(0,0) is zero after
+    // imposesym but kept for fidelity) and the constant-flux pressure
+    const double2 ur = a.u[0][at];
+    double zr = t[2] + (-a.dm.velUp[n]) * ur.x;
+    if (a.const_flux) {
+        double Pr0 = 0.0;
+        for (int j = 0; j <= KL; ++j) Pr0 += a.u[2][(size_t)(g.N - 1 - KL + j) * g.Hp].x * a.dm.dr1[1 * (KL + 1) + j];
+        Pr0 = Pr0 / (-2.0);
+        zr = zr + 4.0 * Pr0 / g.Re;
+    }
+    a.N[0][at] = make_double2(t[0], 0.0);
+    a.N[1][at] = make_double2(t[1], 0.0);
+    a.N[2][at] = make_double2(zr, (-a.dm.velUp[n]) * ur.y);
+}
+
+static size_t mean_smem(int N) { return (size_t)2 * N * 32 * sizeof(double2); }
+__global__ void __launch_bounds__(MEAN_THREADS) k_nl_mean64_part(NLArgs a) { nl_mean64_part_body(a, blockIdx.x); }
+// one warp per radial point
+__global__ void __launch_bounds__(128) k_nl_mean64_fin(NLArgs a) {
+    const int n = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (n < a.g.N) nl_mean64_fin_body(a, n);
+}
 
 // ------------------------------------------------------------------ batched
 // One launch per (stage, transform length) covers the blocks of every pipe
@@ -513,10 +588,30 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_zfwd_b(const NLArgs *__restri
     nl_zfwd_body<ZL, C>(a, pb.y % gx, (pb.y / gx) % a.g.N, pb.y / (gx * a.g.N));
 }
 
-__global__ void k_nl_mean64_batch(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
+__global__ void __launch_bounds__(MEAN_THREADS) k_nl_mean64_part_batch(const NLArgs *__restrict__ args,
+                                                                      const int2 *__restrict__ blk) {
     const int2 pb = blk[blockIdx.x];
     const NLArgs a = args[pb.x];
-    nl_mean64_body(a, pb.y);
+    nl_mean64_part_body(a, pb.y);
+}
+__global__ void __launch_bounds__(128) k_nl_mean64_fin_batch(const NLArgs *__restrict__ args,
+                                                            const int2 *__restrict__ blk) {
+    const int2 pb = blk[blockIdx.x];
+    const NLArgs a = args[pb.x];
+    const int n = pb.y * 4 + (threadIdx.x >> 5);
+    if (n < a.g.N) nl_mean64_fin_body(a, n);
+}
+
+// shared-memory limit of the mean-mode partial-sum kernels (up to N = 128)
+static int mean_attrs() {
+    static bool set = false;
+    if (!set) {
+        const int bytes = (int)mean_smem(128);
+        PF_CUDA(cudaFuncSetAttribute(k_nl_mean64_part, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        PF_CUDA(cudaFuncSetAttribute(k_nl_mean64_part_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        set = true;
+    }
+    return PF_OK;
 }
 
 namespace {
@@ -535,8 +630,9 @@ struct pf_nl_batch {
     int n;
     NLArgs *d_args[2];  // [pointer state]: 0 = as built, 1 = vel/prev swapped
     std::vector<NLGroup> groups[NLB_STAGES];
-    int2 *mean_blk;     // FP64 mean mode of the mixed-precision pipes
-    int nmean;
+    int2 *mean_blk, *fin_blk;  // FP64 mean mode of the mixed-precision pipes: chunks, radial points
+    int nmean, nfin;
+    size_t mean_sm;
     cudaStream_t aux[NLB_MAXG];
     cudaEvent_t fork[NLB_STAGES], join[NLB_STAGES][NLB_MAXG];
 };
@@ -558,6 +654,7 @@ void pf_nl_batch_free(pf_nl_batch *b) {
             if (b->join[st][k]) cudaEventDestroy(b->join[st][k]);
     }
     cudaFree(b->mean_blk);
+    cudaFree(b->fin_blk);
     for (int k = 0; k < NLB_MAXG; ++k)
         if (b->aux[k]) cudaStreamDestroy(b->aux[k]);
     delete b;
@@ -612,12 +709,19 @@ static int nlb_groups(pf_nl_batch *b, pf_ctx *const *pipes, int n) {
             PF_TRY(upload(&b->groups[st].back().blk, map));
         }
     }
-    std::vector<int2> mean;
+    std::vector<int2> mean, fin;
+    b->mean_sm = 0;
     for (int i = 0; i < n; ++i)
-        if (is_mixed(pipes[i]))
-            for (int l = 0; l < pipes[i]->g.N; ++l) mean.push_back(make_int2(i, l));
+        if (is_mixed(pipes[i])) {
+            const Geo &g = pipes[i]->g;
+            for (int l = 0; l < (g.H + 31) / 32; ++l) mean.push_back(make_int2(i, l));
+            for (int l = 0; l < (g.N + 3) / 4; ++l) fin.push_back(make_int2(i, l));
+            b->mean_sm = std::max(b->mean_sm, mean_smem(g.N));
+        }
     b->nmean = (int)mean.size();
-    return upload(&b->mean_blk, mean);
+    b->nfin = (int)fin.size();
+    PF_TRY(upload(&b->mean_blk, mean));
+    return upload(&b->fin_blk, fin);
 }
 
 // Arguments of every pipe in both pointer states, and the per-group maps.
@@ -718,10 +822,13 @@ int pf_nl_batch_launch(pf_nl_batch *b, int state, cudaStream_t st, pf_stage_prof
     if (b->nmean > 0) {
         {
             StageScope ss_(prof, PF_K_ZFWD, st);
-            k_nl_mean64_batch<<<b->nmean, 256, 0, st>>>(args, b->mean_blk);
+            PF_TRY(mean_attrs());
+            k_nl_mean64_part_batch<<<b->nmean, MEAN_THREADS, b->mean_sm, st>>>(args, b->mean_blk);
+            PF_CHECK_LAUNCH();
+            k_nl_mean64_fin_batch<<<b->nfin, 128, 0, st>>>(args, b->fin_blk);
         }
         PF_CHECK_LAUNCH();
-        *nk += 1;
+        *nk += 2;
     }
     return PF_OK;
 }

@@ -726,6 +726,8 @@ struct pf_step_batch {
     StepArgs *d_args[2][2];  // [pointer state after the predictor's swap][mode]
     int2 *tile, *proj, *half;  // (pipe, tile) maps: 32-mode tiles, 128-mode x row tiles, 16-mode tiles
     int ntile, nproj, nhalf;
+    int2 *ldmap[2];            // 32-mode tiles of the pipes whose Helmholtz factors [0] never / [1] pivot
+    int nld[2];
     int maxN;
     bool anypiv;
 };
@@ -736,6 +738,8 @@ void pf_step_batch_free(pf_step_batch *b) {
         for (int m = 0; m < 2; ++m) cudaFree(b->d_args[s][m]);
     cudaFree(b->tile);
     cudaFree(b->half);
+    cudaFree(b->ldmap[0]);
+    cudaFree(b->ldmap[1]);
     cudaFree(b->proj);
     delete b;
 }
@@ -748,7 +752,7 @@ int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
     b->maxN = 0;
     b->anypiv = false;
     std::vector<StepArgs> h(n);
-    std::vector<int2> tile, proj, half;
+    std::vector<int2> tile, proj, half, ldm[2];
     for (int i = 0; i < n; ++i) {
         const Geo &g = pipes[i]->g;
         if (!pf_fused_step_geo_ok(g)) {
@@ -759,6 +763,7 @@ int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
         b->maxN = std::max(b->maxN, g.N);
         b->anypiv |= any_ld_pivoted(pipes[i]);
         for (int t = 0; t < (int)grid1(g.H, TM); ++t) tile.push_back(make_int2(i, t));
+        for (int t = 0; t < (int)grid1(g.H, TM); ++t) ldm[any_ld_pivoted(pipes[i]) ? 1 : 0].push_back(make_int2(i, t));
         for (int t = 0; t < (int)grid1(g.H, HM); ++t) half.push_back(make_int2(i, t));
         for (int t = 0; t < (int)(grid1(g.H, 128) * grid1(g.N, PR)); ++t) proj.push_back(make_int2(i, t));
     }
@@ -779,6 +784,16 @@ int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
         }
     b->ntile = (int)tile.size();
     b->nhalf = (int)half.size();
+    for (int q = 0; q < 2; ++q) {
+        b->nld[q] = (int)ldm[q].size();
+        if (cudaMalloc((void **)&b->ldmap[q], std::max<size_t>(1, ldm[q].size()) * sizeof(int2)) != cudaSuccess ||
+            (!ldm[q].empty() && cudaMemcpy(b->ldmap[q], ldm[q].data(), ldm[q].size() * sizeof(int2),
+                                           cudaMemcpyHostToDevice) != cudaSuccess)) {
+            pf_step_batch_free(b);
+            pf_set_error("batched step: tile map upload failed");
+            return PF_ERR_CUDA;
+        }
+    }
     if (cudaMalloc((void **)&b->half, half.size() * sizeof(int2)) != cudaSuccess ||
         cudaMemcpy(b->half, half.data(), half.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess) {
         pf_step_batch_free(b);
@@ -804,7 +819,6 @@ int pf_step_batch_launch(pf_step_batch *b, int state, int corrector, cudaStream_
                          unsigned long long *nk) {
     PF_TRY(step_attrs());
     const StepArgs *a = b->d_args[state][corrector ? 1 : 0];
-    const int ldsw = b->anypiv ? KV + 1 : KL + 1;
     {
         StageScope ss_(prof, PF_K_STEP, st);
         if (b->maxN <= HR * 4)
@@ -825,7 +839,12 @@ int pf_step_batch_launch(pf_step_batch *b, int state, int corrector, cudaStream_
     PF_CHECK_LAUNCH();
     {
         StageScope ss_(prof, PF_K_LUSOLVE, st);
-        k_solve_ld_batch<<<b->ntile, 192, (size_t)192 * RING * ldsw * sizeof(double), st>>>(a, b->tile);
+        // pipes whose Helmholtz factors never pivot take the narrow ring (more
+        // blocks per SM), the others the wide one
+        for (int q = 0; q < 2; ++q)
+            if (b->nld[q] > 0)
+                k_solve_ld_batch<<<b->nld[q], 192, (size_t)192 * RING * (q ? KV + 1 : KL + 1) * sizeof(double), st>>>(
+                    a, b->ldmap[q]);
     }
     PF_CHECK_LAUNCH();
     {
@@ -833,6 +852,6 @@ int pf_step_batch_launch(pf_step_batch *b, int state, int corrector, cudaStream_
         k_step_final_batch<<<b->ntile, TM * TR, 0, st>>>(a, b->tile);
     }
     PF_CHECK_LAUNCH();
-    *nk += 5;
+    *nk += 4 + (b->nld[0] > 0) + (b->nld[1] > 0);
     return PF_OK;
 }

@@ -91,9 +91,12 @@ def test_batch_staged_launch_count():
     # per step: mean-mode symmetry, the transform stages (one launch per
     # distinct length: zinv and zfwd by Z, theta by Th), 5 step stages, the
     # transform stages again, 5 step stages, the symmetry again, scalar gather
+    # (the Helmholtz solves take a second launch when some pipes' factors
+    # pivot and others' do not)
     cfgs = _cfgs()
     nl = 2 * len({c.Z for c in cfgs}) + len({c.Th for c in cfgs})
-    assert batch.launches() - n0 == 2 * (1 + nl + 5 + nl + 5 + 1 + 1)
+    base = 1 + nl + 5 + nl + 5 + 1 + 1
+    assert batch.launches() - n0 in (2 * base, 2 * (base + 2))
     batch.close()
 
 
