@@ -193,78 +193,104 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+__device__ __forceinline__ void cp_async8s(unsigned saddr, const double *gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(gmem) : "memory");
+}
+
 // dgbtrs ('N', one right-hand side) followed by dtbsv: rhs(n) = rhs[n*rs],
 // solution to out[n*os] (out must not alias rhs).  PIV: LAPACK band with
 // KL+KU superdiagonals in U and pivots pivd[col*Hp+nh] (as doubles); else
-// the pivot-free band with KU = KL.
-template <bool PIV>
+// the pivot-free band with KU = KL.  The ring is strided by the block's TS
+// threads; the column loop is unrolled by RING so every ring slot is a
+// constant shared-memory offset, and the global addresses step by one
+// column per iteration instead of being recomputed.
+template <bool PIV, int TS>
 __device__ __forceinline__ void solve_async(const double *__restrict__ lu, const double *__restrict__ pivd, int N,
                                             int Hp, int nh, const double *__restrict__ rhs, size_t rs, double *out,
-                                            size_t os, double *ring, int ts) {
+                                            size_t os, double *ring) {
     constexpr int KU = PIV ? KV : KL;
     constexpr int SWF = KL + 1 + (PIV ? 1 : 0);  // forward slot: L column, rhs ahead, pivot
     constexpr int SWB = KU + 1;                  // backward slot: U column
     constexpr int SW = SWF > SWB ? SWF : SWB;
-#define LUA(row, col) (lu + ((size_t)(row) * N + (col)) * Hp + nh)
-#define RSLOT(s, q) ring[((s) * SW + (q)) * ts]
-    auto issue_fwd = [&](int j) {
-        if (j < N) {
-            const int s = j % RING;
-            if (j < N - 1) {
+    constexpr unsigned QB = 8u * TS, SB = 8u * TS * SW;  // bytes between values / slots
+    const size_t rowst = (size_t)N * Hp;                 // doubles between band rows
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(ring);
+#define RSLOT(s, q) ring[((s) * SW + (q)) * TS]
+    // forward: column j needs L(KV+1+i, j), i < KL, rhs(j+KL+1) and its pivot
+    const double *Lj = lu + (size_t)(KV + 1) * rowst + nh;
+    const double *Pj = PIV ? pivd + nh : nullptr;
+    const double *Rj = rhs + (size_t)(KL + 1) * rs;
+    int jj = 0;  // next column to stage
+    auto issue_fwd = [&](int s) {
+        if (jj < N) {
+            if (jj < N - 1) {
 #pragma unroll
-                for (int i = 0; i < KL; ++i) cp_async8(&RSLOT(s, i), LUA(KV + 1 + i, j));
-                if (PIV) cp_async8(&RSLOT(s, KL + 1), pivd + (size_t)j * Hp + nh);
+                for (int i = 0; i < KL; ++i) cp_async8s(sbase + s * SB + i * QB, Lj + i * rowst);
+                if (PIV) cp_async8s(sbase + s * SB + (KL + 1) * QB, Pj);
             }
-            if (j + KL + 1 < N) cp_async8(&RSLOT(s, KL), rhs + (size_t)(j + KL + 1) * rs);
+            if (jj + KL + 1 < N) cp_async8s(sbase + s * SB + KL * QB, Rj);
         }
         cp_async_commit();
+        ++jj;
+        Lj += Hp;
+        if (PIV) Pj += Hp;
+        Rj += rs;
     };
     double w[KL + 1];
 #pragma unroll
     for (int i = 0; i <= KL; ++i) w[i] = (i < N) ? rhs[(size_t)i * rs] : 0.0;
 #pragma unroll
-    for (int j = 0; j < RING; ++j) issue_fwd(j);
-    for (int j = 0; j < N; ++j) {
-        cp_async_wait<RING - 1>();
-        const int s = j % RING;
-        const double ahead = (j + KL + 1 < N) ? RSLOT(s, KL) : 0.0;
-        if (j < N - 1) {
-            if (PIV) {
-                const int p = (int)RSLOT(s, KL + 1);
+    for (int s = 0; s < RING; ++s) issue_fwd(s);
+    double *Oj = out;
+    for (int j0 = 0; j0 < N; j0 += RING) {
 #pragma unroll
-                for (int i = 1; i <= KL; ++i)
-                    if (p == i) {
-                        const double t = w[0];
-                        w[0] = w[i];
-                        w[i] = t;
+        for (int s = 0; s < RING; ++s) {
+            const int j = j0 + s;
+            if (j < N) {
+                cp_async_wait<RING - 1>();
+                const double ahead = (j + KL + 1 < N) ? RSLOT(s, KL) : 0.0;
+                if (j < N - 1) {
+                    if (PIV) {
+                        const int p = (int)RSLOT(s, KL + 1);
+#pragma unroll
+                        for (int i = 1; i <= KL; ++i)
+                            if (p == i) {
+                                const double t = w[0];
+                                w[0] = w[i];
+                                w[i] = t;
+                            }
                     }
+                    const double bj = w[0];
+#pragma unroll
+                    for (int i = 1; i <= KL; ++i)
+                        if (j + i < N) w[i] = fma(-RSLOT(s, i - 1), bj, w[i]);
+                }
+                *Oj = w[0];
+                Oj += os;
+#pragma unroll
+                for (int i = 0; i < KL; ++i) w[i] = w[i + 1];
+                w[KL] = ahead;
+                issue_fwd(s);
             }
-            const double bj = w[0];
-#pragma unroll
-            for (int i = 1; i <= KL; ++i)
-                if (j + i < N) w[i] = fma(-RSLOT(s, i - 1), bj, w[i]);
         }
-        out[(size_t)j * os] = w[0];
-#pragma unroll
-        for (int i = 0; i < KL; ++i) w[i] = w[i + 1];
-        w[KL] = ahead;
-        issue_fwd(j + RING);
     }
     cp_async_wait<0>();
-    // back substitution; y (this thread's forward output) is read through a
-    // four-deep register queue, with streaming loads: each value is read once
-    // and then overwritten by the solution
-    auto issue_bwd = [&](int t) {  // step t handles column N-1-t
-        const int j = N - 1 - t;
-        if (j >= 0) {
-            const int s = t % RING;
+    // back substitution: column j needs U(KV-i, j), i <= KU; y (this thread's
+    // forward output) is read through a four-deep register queue, with
+    // streaming loads: each value is read once and then overwritten
+    const double *Uj = lu + (size_t)KV * rowst + (size_t)(N - 1) * Hp + nh;
+    int tt = 0;  // next step to stage (step t handles column N-1-t)
+    auto issue_bwd = [&](int s) {
+        if (tt < N) {
 #pragma unroll
-            for (int i = 0; i <= KU; ++i) cp_async8(&RSLOT(s, i), LUA(KV - i, j));
+            for (int i = 0; i <= KU; ++i) cp_async8s(sbase + s * SB + i * QB, Uj - i * rowst);
         }
         cp_async_commit();
+        ++tt;
+        Uj -= Hp;
     };
 #pragma unroll
-    for (int t = 0; t < RING; ++t) issue_bwd(t);
+    for (int s = 0; s < RING; ++s) issue_bwd(s);
     double v[KU + 1];
 #pragma unroll
     for (int i = 0; i <= KU; ++i) v[i] = (N - 1 - i >= 0) ? __ldcs(out + (size_t)(N - 1 - i) * os) : 0.0;
@@ -275,32 +301,38 @@ __device__ __forceinline__ void solve_async(const double *__restrict__ lu, const
         const int r = N - 1 - KU - 1 - q;
         yq[q] = (r >= 0) ? __ldcs(out + (size_t)r * os) : 0.0;
     }
-    for (int t = 0; t < N; ++t) {
-        const int j = N - 1 - t;
-        cp_async_wait<RING - 1>();
-        const int s = t % RING;
-        const double ahead = yq[0];
+    double *Xj = out + (size_t)(N - 1) * os;
+    for (int t0 = 0; t0 < N; t0 += RING) {
 #pragma unroll
-        for (int q = 0; q < QY - 1; ++q) yq[q] = yq[q + 1];
-        {
-            const int r = j - KU - 1 - QY;
-            yq[QY - 1] = (r >= 0) ? __ldcs(out + (size_t)r * os) : 0.0;
+        for (int s = 0; s < RING; ++s) {
+            const int t = t0 + s;
+            if (t < N) {
+                const int j = N - 1 - t;
+                cp_async_wait<RING - 1>();
+                const double ahead = yq[0];
+#pragma unroll
+                for (int q = 0; q < QY - 1; ++q) yq[q] = yq[q + 1];
+                {
+                    const int r = j - KU - 1 - QY;
+                    yq[QY - 1] = (r >= 0) ? __ldcs(out + (size_t)r * os) : 0.0;
+                }
+                double x = v[0];
+                if (x != 0.0) {
+                    x = x / RSLOT(s, 0);
+#pragma unroll
+                    for (int i = 1; i <= KU; ++i)
+                        if (j - i >= 0) v[i] = fma(-x, RSLOT(s, i), v[i]);
+                }
+                *Xj = x;
+                Xj -= os;
+#pragma unroll
+                for (int i = 0; i < KU; ++i) v[i] = v[i + 1];
+                v[KU] = (j - KU - 1 >= 0) ? ahead : 0.0;
+                issue_bwd(s);
+            }
         }
-        double x = v[0];
-        if (x != 0.0) {
-            x = x / RSLOT(s, 0);
-#pragma unroll
-            for (int i = 1; i <= KU; ++i)
-                if (j - i >= 0) v[i] = fma(-x, RSLOT(s, i), v[i]);
-        }
-        out[(size_t)j * os] = x;
-#pragma unroll
-        for (int i = 0; i < KU; ++i) v[i] = v[i + 1];
-        v[KU] = (j - KU - 1 >= 0) ? ahead : 0.0;
-        issue_bwd(t + RING);
     }
     cp_async_wait<0>();
-#undef LUA
 #undef RSLOT
 }
 
@@ -319,7 +351,7 @@ __device__ __forceinline__ void solve_pnp_body(const StepArgs &a, int bx) {
         for (int n = 0; n < g.N; ++n) out[n * st] = 0.0;
         return;
     }
-    solve_async<true>(a.lnp, a.pivd, g.N, g.Hp, nh, rhs, st, out, st, ring2 + threadIdx.x, blockDim.x);
+    solve_async<true, 64>(a.lnp, a.pivd, g.N, g.Hp, nh, rhs, st, out, st, ring2 + threadIdx.x);
 }
 
 // S3: rhs - rt2pm(grad p) (velocity.f90:232-236) with zero boundary rows
@@ -395,9 +427,9 @@ __device__ __forceinline__ void solve_ld_body(const StepArgs &a, int bx) {
     double *out = reinterpret_cast<double *>(pick3(a.v, sys)) + 2 * (size_t)nh + part;
     const double *lu = sys == 0 ? a.ldp : sys == 1 ? a.ldm : a.ldz;
     if (pick3(a.ldpiv, sys))  // pivoting band (low Re, small dt or very clustered meshes)
-        solve_async<true>(lu, pick3(a.pivld, sys), g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x, blockDim.x);
+        solve_async<true, 192>(lu, pick3(a.pivld, sys), g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x);
     else
-        solve_async<false>(lu, nullptr, g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x, blockDim.x);
+        solve_async<false, 192>(lu, nullptr, g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x);
 }
 
 // ------------------------------------------------------------------- S5
