@@ -122,11 +122,16 @@ class ClockSampler:
 
 
 def cpu_baseline(workload: str, nsample: int):
-    """Time the FP64 oracle (CPU restatement of the reference step) on a
-    bounded sample of the workload: one step of each of the first `nsample`
-    pipes (batched) or `nsample` steps of the single pipe."""
+    """Time the CPU restatement of the reference step (oracle/pipeflow_cpu.cpp:
+    C++, OpenMP over modes and radial points, every host thread) on a bounded
+    sample of the workload: one step of each of the first `nsample` pipes of
+    the mix after one warm-up step (batched), or `nsample` steps of the single
+    pipe.  The set-up (mesh, factors, influence matrices) comes from the numpy
+    oracle and is not timed."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import pipeflow_oracle as O
+    import pipeflow_cpu as PC
+    threads = PC.threads()
     if workload == "batched":
         cfgs = batched_configs()[:nsample]
         pipes = []
@@ -134,26 +139,30 @@ def cpu_baseline(workload: str, nsample: int):
             o = O.Pipe(O.PipeConfig(**d))
             o.vel_matrices()
             o.set_state(*O.seeded_state(o, 1000 + i, 1e-3))
-            pipes.append(o)
+            c = PC.CpuPipe(o)
+            c.timestep()
+            pipes.append(c)
         t0 = time.perf_counter()
-        for o in pipes:
-            o.timestep()
+        for c in pipes:
+            c.timestep()
         dt = time.perf_counter() - t0
-        return {"value": len(pipes) / dt, "unit": "timesteps/s", "cores": 1, "kind": "port",
-                "sample": f"one main-loop step of each of the first {len(pipes)} pipes of the 64-pipe mix, "
-                          f"FP64 numpy/scipy oracle, after matrices and seeding"}
+        return {"value": len(pipes) / dt, "unit": "timesteps/s", "cores": threads, "kind": "port",
+                "sample": f"one main-loop step of each of the first {len(pipes)} pipes of the 64-pipe mix in FP64, "
+                          f"C++/OpenMP restatement of the reference step on {threads} host threads, after one "
+                          f"warm-up step (set-up not timed)"}
     w = SINGLE[workload]
     o = O.Pipe(O.PipeConfig(**{k: w[k] for k in PHYS}))
     o.vel_matrices()
     o.set_state(*O.seeded_state(o, w["seed"], w["energy"]))
-    o.timestep()
+    c = PC.CpuPipe(o)
+    c.timestep()
     t0 = time.perf_counter()
     for _ in range(nsample):
-        o.timestep()
+        c.timestep()
     dt = time.perf_counter() - t0
-    return {"value": nsample / dt, "unit": "timesteps/s", "cores": 1, "kind": "port",
-            "sample": f"{nsample} steps of the FP64 numpy/scipy oracle on the same pipe "
-                      f"(after matrices, seed and 1 warm-up step; no spin-up)"}
+    return {"value": nsample / dt, "unit": "timesteps/s", "cores": threads, "kind": "port",
+            "sample": f"{nsample} steps of the C++/OpenMP restatement of the reference step on {threads} host "
+                      f"threads (after matrices, seed and 1 warm-up step; no spin-up)"}
 
 
 def read_traffic(kernel: str, workload: str):
@@ -422,6 +431,18 @@ def run_batched(args, torch, P, dist, world, rank, local):
         extra["mixed_vs_fp64"] = mixed_error(P, cfgs[0], seeds[0], args.err_steps)
         if args.with_serve:
             extra["serve"] = run_serve(args, P, local, plain)
+        if args.with_cfg2 and not args.no_cpu_baseline:
+            # config-1: the plain FP64 drop-in on one pipe against the CPU
+            # restatement of the reference step on every host thread
+            sub = argparse.Namespace(**vars(args))
+            sub.workload, sub.spinup, sub.steps = "cfg1", 0, 200
+            r1 = run_single(sub, torch, P, None, 1, 0, local)
+            gpu1 = sub.steps / (r1["ms"] / 1e3)
+            cpu1 = cpu_baseline("cfg1", 10)
+            extra["cfg1"] = {"gpu_plain": gpu1, "cpu": cpu1["value"], "cpu_cores": cpu1["cores"],
+                             "unit": "timesteps/s", "gpu_over_cpu": gpu1 / cpu1["value"],
+                             "what": "N=40 K=24 M=16 FP64, one pipe: pf_timestep (CUDA graph) vs the "
+                                     "C++/OpenMP CPU restatement"}
         if args.with_cfg2:
             sub = argparse.Namespace(**vars(args))
             sub.workload, sub.spinup, sub.steps = "cfg2", args.cfg2_spinup, args.cfg2_steps
@@ -473,7 +494,7 @@ def main():
     ap.add_argument("--workload", default="batched", choices=["batched", "cfg2", "cfg1"])
     ap.add_argument("--pipes", type=int, default=64)
     ap.add_argument("--spinup", type=int, default=None)
-    ap.add_argument("--ref-steps", type=int, default=4)
+    ap.add_argument("--ref-steps", type=int, default=16)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--plain-pipes", type=int, default=64)
     ap.add_argument("--err-steps", type=int, default=100)
