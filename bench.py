@@ -401,11 +401,12 @@ def run_batched(args, torch, P, dist, world, rank, local):
     e0, e1 = dev_timer(torch, master)
     e0.record(master)
     for _ in range(ne):
-        for p, (_, ptrs) in zip(batch.pipes, host):
+        for p, (_, ptrs) in zip(batch.pipes, host):  # queued on each pipe's stream
             P.api._check(p.lib.pf_vel_set_state(p.ctx, *ptrs))
-        batch.step(1)
+        batch.step(1)  # waits for the uploads on the device, returns after the step
         for p, (_, ptrs) in zip(batch.pipes, host):
-            P.api._check(p.lib.pf_vel_get_state(p.ctx, *ptrs))
+            P.api._check(p.lib.pf_vel_get_state_async(p.ctx, *ptrs))
+        batch.sync()
     e1.record(master)
     master.synchronize()
     e2e_ms = e0.elapsed_time(e1)

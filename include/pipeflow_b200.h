@@ -199,6 +199,12 @@ int pf_vel_set_state(pf_ctx *ctx, const double *ur_re, const double *ur_im,
                      const double *uz_re, const double *uz_im);
 int pf_vel_get_state(pf_ctx *ctx, double *ur_re, double *ur_im,
                      double *ut_re, double *ut_im, double *uz_re, double *uz_im);
+/* The same copy queued on the context's stream without waiting (the arrays
+ * are complete once pf_ctx_sync returns; page-locked arrays let the copies of
+ * many contexts overlap).  No separate reference routine: the host side of
+ * io.f90's state access, batched. */
+int pf_vel_get_state_async(pf_ctx *ctx, double *ur_re, double *ur_im, double *ut_re,
+                           double *ut_im, double *uz_re, double *uz_im);
 int pf_vel_get_scalars(const pf_ctx *ctx, double *Pr0, double *nu);
 int pf_vel_imposesym(pf_ctx *ctx);                                  /* :61-74 */
 int pf_vel_matrices(pf_ctx *ctx);                                   /* :120-146 */

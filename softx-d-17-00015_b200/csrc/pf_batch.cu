@@ -527,6 +527,12 @@ extern "C" int pf_batch_step(pf_batch *b, int nsteps, int orbit, long long *corr
             }
         }
         const int p = b->pipes[0]->parity;
+        // work the caller queued on a pipe's own stream (set_state, uploads)
+        // comes before the batch's launches on the master stream
+        for (int i = 0; i < b->n; ++i) {
+            PF_CUDA(cudaEventRecord(b->join[i], b->pipes[i]->stream));
+            PF_CUDA(cudaStreamWaitEvent(b->master, b->join[i], 0));
+        }
         if (b->kind == 1 && (b->fresh || !b->use_graphs)) {
             // launched directly: the first step after a build (it also sets
             // the kernels' shared-memory limits outside any capture) and

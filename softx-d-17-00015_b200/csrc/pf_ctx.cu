@@ -403,6 +403,21 @@ static int coll_upload(pf_ctx *ctx, double2 *dst, const double *re, const double
     return PF_OK;
 }
 
+static int coll_download_async(pf_ctx *ctx, const double2 *src, double *re, double *im) {
+    const Geo &g = ctx->g;
+    const size_t nb = (size_t)g.N * g.H * sizeof(double);
+    double *stage = (double *)ctx->s[7].d;  // reused in stream order by the next field
+    dim3 grid(grid1(g.Hp, 32), grid1(g.N, 32)), block(32, 8);
+    {
+        ProfScope ps_(ctx, PF_K_EW);
+        k_coll_to_host<<<grid, block, 0, ctx->stream>>>(src, stage, stage + (size_t)g.N * g.H, g.N, g.H, g.Hp);
+    }
+    PF_LAUNCHED(ctx);
+    PF_CUDA(cudaMemcpyAsync(re, stage, nb, cudaMemcpyDeviceToHost, ctx->stream));
+    PF_CUDA(cudaMemcpyAsync(im, stage + (size_t)g.N * g.H, nb, cudaMemcpyDeviceToHost, ctx->stream));
+    return PF_OK;
+}
+
 static int coll_download(pf_ctx *ctx, const double2 *src, double *re, double *im) {
     const Geo &g = ctx->g;
     const size_t nb = (size_t)g.N * g.H * sizeof(double);
@@ -529,6 +544,18 @@ extern "C" int pf_vel_get_state(pf_ctx *ctx, double *ur_re, double *ur_im, doubl
     PF_TRY(coll_download(ctx, ctx->vel[0].d, ur_re, ur_im));
     PF_TRY(coll_download(ctx, ctx->vel[1].d, ut_re, ut_im));
     PF_TRY(coll_download(ctx, ctx->vel[2].d, uz_re, uz_im));
+    return PF_OK;
+}
+
+// As pf_vel_get_state, without waiting: the copies are queued on the
+// context's stream and the host arrays are filled once pf_ctx_sync returns.
+// The host arrays should be page-locked for the copies to overlap other work.
+extern "C" int pf_vel_get_state_async(pf_ctx *ctx, double *ur_re, double *ur_im, double *ut_re, double *ut_im,
+                                      double *uz_re, double *uz_im) {
+    PF_ARG(ctx && ur_re && ur_im && ut_re && ut_im && uz_re && uz_im, "null argument");
+    PF_TRY(coll_download_async(ctx, ctx->vel[0].d, ur_re, ur_im));
+    PF_TRY(coll_download_async(ctx, ctx->vel[1].d, ut_re, ut_im));
+    PF_TRY(coll_download_async(ctx, ctx->vel[2].d, uz_re, uz_im));
     return PF_OK;
 }
 

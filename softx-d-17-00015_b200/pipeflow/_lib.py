@@ -108,6 +108,7 @@ _SIGS = {
     "pf_vel_phys": [P, I, PP],
     "pf_vel_set_state": [P, DP, DP, DP, DP, DP, DP],
     "pf_vel_get_state": [P, DP, DP, DP, DP, DP, DP],
+    "pf_vel_get_state_async": [P, DP, DP, DP, DP, DP, DP],
     "pf_vel_get_scalars": [P, DP, DP],
     "pf_vel_imposesym": [P],
     "pf_vel_matrices": [P],

@@ -177,3 +177,45 @@ def test_fused_transform_nonlinear_matches_oracle():
     g.vel_transform_nonlinear()
     for i, ref in enumerate((o.vel_Nr, o.vel_Nt, o.vel_Nz)):
         assert rel_coll(from_dev(g.vel_field(3 + i)), ref) < 1e-12
+
+
+def test_set_state_then_batch_step_is_ordered():
+    """States uploaded on the pipes' own streams right before a batch step are
+    the ones the step reads (the step waits for the uploads on the device), and
+    the asynchronous download returns the stepped states after a sync."""
+    import ctypes as C
+    import pipeflow as P
+    cfgs = _cfgs()
+    batch = P.Batch(cfgs)
+    batch.matrices()
+    for i, bp in enumerate(batch.pipes):
+        _seed(bp, i)
+    batch.step(3)  # graphs captured for both parities
+    fresh = []
+    for i, c in enumerate(cfgs):
+        tmp = P.Pipe(c)
+        P.seeded_state(tmp, 500 + i, 1e-3)
+        fresh.append(tmp.get_state())
+        tmp.close()
+    for bp, st in zip(batch.pipes, fresh):
+        bp.set_state(*st)
+    batch.step(2)
+    outs = []
+    for bp in batch.pipes:
+        arrs = [np.empty((bp.H, bp.N)) for _ in range(6)]
+        ptrs = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
+        assert bp.lib.pf_vel_get_state_async(bp.ctx, *ptrs) == 0
+        outs.append(arrs)
+    batch.sync()
+    for c, st, arrs in zip(cfgs, fresh, outs):
+        ap = P.Pipe(c)
+        ap.vel_matrices()
+        ap.set_state(*st)
+        ap.timestep()
+        ap.timestep()
+        got = [np.ascontiguousarray(a.T) for a in arrs]
+        want = [x for f in ap.get_state() for x in f]
+        for g, w in zip(got, want):
+            assert np.array_equal(g, w)
+        ap.close()
+    batch.close()
