@@ -230,6 +230,32 @@ int pf_timestep(pf_ctx *ctx, int *ncorr);
 /* nsteps passes of steporbit's body (newton.f90:740-762): exactly one
  * corrector per step, no adaptive dt, no shift. */
 int pf_steporbit(pf_ctx *ctx, int nsteps);
+
+/* ------------------------------------------------------- orbit vectors */
+/* Device side of the Newton-Krylov orbit search (newton.f90).  A vector
+ * holds pf_orbit_vec_len = 8 + 6*N*H doubles in device memory: x[0..2] the
+ * theta shift, z shift and period (each divided by scaleT), x[3] the
+ * continuation parameter, x[4..7] unused, and from x[8] on the scaled state
+ * (mode-major, then radial point, then ur/ut/uz Re/Im).  The calls work
+ * through the context's velocity fields (vel_ur, vel_ut, vel_uz), as the
+ * reference's routines do, and leave them holding the last state handled. */
+int pf_orbit_set_scales(pf_ctx *ctx, const double *scaleU, double scaleT); /* newton.f90:272-305 */
+int pf_orbit_vec_len(const pf_ctx *ctx, long long *n);                     /* newton.f90:36 */
+int pf_orbit_rtz2vec(pf_ctx *ctx, double *v);                              /* newton.f90:567-602 */
+int pf_orbit_vec2rtz(pf_ctx *ctx, const double *v);                        /* newton.f90:608-643 */
+/* dotprod(n_,a,b) (newton.f90:652-672): n_ = -1 skips x[0..7].  The sum
+ * order is fixed, so equal inputs give equal results.  Synchronises. */
+int pf_orbit_dotprod(pf_ctx *ctx, int n_, const double *a, const double *b, double *out);
+/* getshiftdir(i,n,x,s), i = 1 (theta) or 2 (z) (newton.f90:533-561); s[0..7]
+ * are not written. */
+int pf_orbit_shiftdir(pf_ctx *ctx, int i, const double *x, double *s);
+/* steporbit(ndts,x,y) without parameter continuation or output files
+ * (newton.f90:721-831): y[8:] = the state ndts steps on from x, shifted back
+ * by (x[0], x[1])*scaleT when ndts != 1; y[0..7] are not written.  With
+ * ndts != 1, dt = x[2]*scaleT/ndts, vel_matrices runs first, and time and
+ * step count advance; a single step leaves dt, time and step count as they
+ * were.  y may equal x.  Returns PF_ERR_CONVERGE as pf_steporbit does. */
+int pf_orbit_step(pf_ctx *ctx, int ndts, const double *x, double *y);
 /* Perturbation energy and friction diagnostics of io.f90:501-514, 627-639. */
 int pf_diag_energy(pf_ctx *ctx, double *E);
 int pf_diag_friction(pf_ctx *ctx, double *Ub, double *Uc, double *Ufr);

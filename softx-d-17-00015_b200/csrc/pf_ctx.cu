@@ -188,6 +188,7 @@ static int ctx_init(pf_ctx *ctx, const pf_config *cfg, int device) {
     PF_TRY(pf_alloc(ctx, (void **)&ctx->Ainv, (size_t)16 * g.Hp * sizeof(double)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->Ui, (size_t)N * sizeof(double)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->red, (size_t)(3 * N + g.Hp + 64) * sizeof(double)));
+    PF_TRY(pf_alloc(ctx, (void **)&ctx->orbit_red, (size_t)(ORBIT_DOT_BLOCKS + 1) * sizeof(double)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->cflmax, (size_t)3 * N * sizeof(unsigned long long)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->mpart, (size_t)((g.H + 31) / 32) * N * 3 * sizeof(double)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->anypiv, sizeof(int)));

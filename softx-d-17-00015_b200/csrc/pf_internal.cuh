@@ -164,6 +164,10 @@ struct pf_ctx {
     double *Ui;          // flux influence vector [N]
     double *red;         // reduction scratch (>= 3*N + H doubles)
     double *mpart;       // FP64 mean-mode partial sums [ceil(H/32)][N][3]
+    // Newton-Krylov vectors (newton.f90:36-37): scaleU, scaleT, dot partials
+    double orbit_scaleU[3], orbit_scaleT;
+    bool orbit_set;
+    double *orbit_red;   // ORBIT_DOT_BLOCKS + 1 doubles
     unsigned long long *cflmax;  // 3*N CFL maxima of the last fused transform
     bool cfl_fused;              // cflmax is current (else use vel_r/t/z)
     int *anypiv;         // per LU set: 1 if dgbtf2 swapped any row
@@ -253,6 +257,9 @@ __device__ __forceinline__ int fdiv(int x, int d, float inv) {
     else if (r >= d) ++q;
     return q;
 }
+
+// partial sums of pf_orbit_dotprod (a fixed count keeps the sum order fixed)
+#define ORBIT_DOT_BLOCKS 256
 
 inline unsigned grid1(long long n, int block) {
     return (unsigned)((n + block - 1) / block);

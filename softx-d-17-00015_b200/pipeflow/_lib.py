@@ -121,6 +121,13 @@ _SIGS = {
     "pf_vel_influence_download": [P, DP, DP],
     "pf_timestep": [P, IP],
     "pf_steporbit": [P, I],
+    "pf_orbit_set_scales": [P, DP, D],
+    "pf_orbit_vec_len": [P, C.POINTER(C.c_longlong)],
+    "pf_orbit_rtz2vec": [P, P],
+    "pf_orbit_vec2rtz": [P, P],
+    "pf_orbit_dotprod": [P, I, P, P, DP],
+    "pf_orbit_shiftdir": [P, I, P, P],
+    "pf_orbit_step": [P, I, P, P],
     "pf_diag_energy": [P, DP],
     "pf_diag_friction": [P, DP, DP, DP],
     "pf_batch_create": [I, C.POINTER(pf_config), I, PP],

@@ -200,6 +200,7 @@ class Pipe:
     def __init__(self, cfg: PipeConfig, device: int = -1, _handle=None):
         self.lib = L.load()
         self.cfg = cfg
+        self.device = device  # -1: the device current at creation
         self._owned = _handle is None
         self.ctx = None
         if _handle is None:

@@ -1,0 +1,517 @@
+"""Newton-Krylov search for relative periodic orbits (newton.f90 with
+NewtonHook.f90 and GMRESm.f90) over the device timestep.
+
+The time-T map, the state <-> vector scaling, the shift directions and the
+dot products run on the GPU through the C ABI (pf_orbit_*); the Krylov basis
+and every Newton vector stay in device memory as float64 torch tensors.  The
+small dense work -- the least-squares solve of the Hessenberg system (dgelsy)
+and the hookstep's SVD (dgesvd) -- runs on the host through scipy's LAPACK,
+as the reference keeps it in LAPACK.
+
+Entry points, named after the reference's routines:
+
+    orb = Orbit(pipe, ndts=[100], shifts=[(0.0, sz, T)])   # shifts.in
+    orb.get_scales()                 # newton.f90:272-305 (after the state is set)
+    orb.load_ms_states()             # newton.f90:311-350 (shooting points by stepping)
+    orb.search_sz()                  # newton.f90:356-394
+    res = orb.solve(m=150, nits=100, rel_err=3e-6, delta=-1.0, mndl=1e-7,
+                    mxdl=1e7, gtol=1e-3)     # the main program's call of newtonhook
+
+plus getrhs / multJ / multA / steporbit / dotprod / dotprod_ms / getshiftdir /
+rtz2vec / vec2rtz on device vectors.  Parameter continuation (Ctnu), the
+Arnoldi eigenvalue step and the output files are not included.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.linalg
+import torch
+
+from . import _lib as L
+from .api import Pipe, PipeflowError, _check
+
+
+def _ptr(t: torch.Tensor) -> int:
+    return t.data_ptr()
+
+
+# ---------------------------------------------------------------------------
+# GMRES with hookstep (GMRESm.f90) on device vectors
+# ---------------------------------------------------------------------------
+def hookstep(j: int, h: np.ndarray, beta: float, delta: float):
+    """GMRESm.f90:119-153: the y that gives the hookstep of size delta in the
+    Krylov space of dimension j, and the residual that it predicts."""
+    a = h[:j + 1, :j].copy()
+    u, s, vt = scipy.linalg.svd(a, full_matrices=True, lapack_driver="gesvd")
+    p = beta * u[0, :j]
+    mu = max(s[j - 1] * s[j - 1] * 1e-6, 1e-99)
+    qn = 1e99
+    while qn > delta:
+        mu = mu * 1.1
+        q = p * s / (mu + s * s)
+        qn = math.sqrt(float(np.dot(q, q)))
+    y = q @ vt
+    pp = -(h[:j + 1, :j] @ y)
+    pp[0] += beta
+    return y, math.sqrt(float(np.dot(pp, pp)))
+
+
+def _least_squares(hj: np.ndarray, rhs: np.ndarray) -> np.ndarray:
+    """dgelsy on the (j+1) x j Hessenberg system (GMRESm.f90:82-85), full
+    rank unless a column is exactly dependent."""
+    y, *_ = scipy.linalg.lstsq(hj, rhs, cond=1e-300, lapack_driver="gelsy")
+    return y
+
+
+class GMRES:
+    """gmresm (GMRESm.f90:27-113).  The Krylov basis v (m+1 vectors) lives
+    on the vectors' device; h, beta and j are kept between calls, so that
+    info=2 recomputes the hookstep for a new trust region without new
+    matrix-vector products."""
+
+    def __init__(self, m: int, n: int, like: torch.Tensor):
+        self.m, self.n = m, n
+        self.h = np.zeros((m + 1, m))
+        self.v = torch.zeros((m + 1, n), dtype=like.dtype, device=like.device)
+        self.beta = 0.0
+        self.j = 0
+
+    def _combine(self, y: np.ndarray, j: int) -> torch.Tensor:
+        yt = torch.as_tensor(y[:j], dtype=self.v.dtype).to(self.v.device, non_blocking=False)
+        return yt @ self.v[:j]
+
+    def solve(self, x, b, matvec, dot, res, delta, its, info):
+        """Returns (x, res, delta, its, info) as gmresm leaves its arguments:
+        x the solution (hookstep if delta > 0), res the residual reached,
+        delta the residual the hookstep predicts, its the iterations taken,
+        info 0 converged / 1 breakdown / 2 iteration limit."""
+        m = self.m
+        if info == 2:
+            y, delta = hookstep(self.j, self.h, self.beta, delta)
+            return self._combine(y, self.j), res, delta, its, 0
+        tol = res
+        imx = its
+        its = 0
+        self.v.zero_()
+        while True:
+            res_ = 1e99
+            stgn = 1.0 - 1e-14
+            beta = math.sqrt(dot(x, x))
+            w = torch.zeros_like(b) if beta == 0.0 else matvec(x)
+            w = b - w
+            beta = math.sqrt(dot(w, w))
+            self.beta = beta
+            self.v[0] = w / beta
+            self.h[:] = 0.0
+            for j in range(1, m + 1):
+                self.j = j
+                its += 1
+                w = matvec(self.v[j - 1].clone())
+                for i in range(1, j + 1):
+                    hij = dot(w, self.v[i - 1])
+                    self.h[i - 1, j - 1] = hij
+                    w = w - hij * self.v[i - 1]
+                self.h[j, j - 1] = math.sqrt(dot(w, w))
+                self.v[j] = w / self.h[j, j - 1]
+                p = np.zeros(j + 1)
+                p[0] = beta
+                y = _least_squares(self.h[:j + 1, :j], p)
+                p = -(self.h[:j + 1, :j] @ y)
+                p[0] += beta
+                res = math.sqrt(float(np.dot(p, p)))
+                done = res <= tol or its == imx or res > res_
+                if done or j == m:
+                    if delta > 0.0:
+                        y, delta = hookstep(j, self.h, beta, delta)
+                    x = x + self._combine(y, j)
+                    if its == imx:
+                        info = 2
+                    if res > res_:
+                        info = 1
+                    if res <= tol:
+                        info = 0
+                    if done:
+                        return x, res, delta, its, info
+                    break  # restart with the new x
+                res_ = res * stgn
+
+
+@dataclass
+class NewtonResult:
+    """newtonhook's exit state: the iterate, its residual vector and norm,
+    the trust region, Newton and GMRES iteration counts, and info
+    (0 converged, 2 iteration limit, 3 trust region below mndl)."""
+    x: torch.Tensor
+    fx: torch.Tensor
+    tol: float
+    delta: float
+    nits: int
+    gits: int
+    info: int
+    history: list = field(default_factory=list)
+
+
+class NewtonState:
+    """The newton module's variables (NewtonHook.f90:39-45)."""
+    new_x = None
+    new_fx = None
+    new_tol = 0.0
+    new_del = 0.0
+    new_nits = 0
+    new_gits = 0
+
+
+def newtonhook(f, df, dp, x0, m, gtol, tol, delta, mndl, mxdl, nits, state: NewtonState | None = None, sub=None):
+    """Newton iteration with GMRES hooksteps (NewtonHook.f90:46-180) for
+    f(x) = 0.  f and df map vectors to vectors (df is the Jacobian with its
+    constraint rows), dp is the dot product, sub() runs after every accepted
+    iteration; state.new_x / state.new_fx hold the current iterate while f
+    and df run."""
+    n = x0.numel()
+    st = state if state is not None else NewtonState()
+    st.new_x = x0.clone()
+    st.new_nits = 0
+    st.new_gits = 0
+    st.new_del = delta
+    mxdl_ = mxdl
+    ginfo = 0
+    gm = GMRES(m, n, x0)
+    st.new_fx = f(st.new_x)
+    st.new_tol = math.sqrt(dp(st.new_fx, st.new_fx))
+    if delta < 0.0:
+        st.new_del = st.new_tol / 10.0
+        mxdl_ = 1e99
+    hist = [(st.new_nits, st.new_gits, st.new_tol, st.new_del)]
+    if sub:
+        sub()
+    x_, fx_, tol_ = st.new_x.clone(), st.new_fx.clone(), st.new_tol
+    tol__ = 1e99
+    x__ = fx__ = None
+    del__ = 0.0
+
+    def result(info):
+        return NewtonResult(st.new_x, st.new_fx, st.new_tol, st.new_del, st.new_nits, st.new_gits, info, hist)
+
+    if st.new_tol < tol:
+        return result(0)
+    while True:
+        if st.new_del < mndl:
+            return result(3)
+        s = torch.zeros_like(x0)
+        gres = gtol * st.new_tol
+        gdel = st.new_del
+        if ginfo != 2:
+            st.new_gits = m
+        s, gres, gdel, st.new_gits, ginfo = gm.solve(s, fx_, df, dp, gres, gdel, st.new_gits, ginfo)
+        ginfo = 0
+        st.new_x = x_ - s
+        st.new_fx = f(st.new_x)
+        st.new_tol = math.sqrt(dp(st.new_fx, st.new_fx))
+        snrm = math.sqrt(dp(s, s))
+        ared = tol_ - st.new_tol
+        pred = tol_ - gdel
+        if st.new_tol > tol__:  # accept the previous, better step
+            st.new_x, st.new_fx, st.new_tol, st.new_del = x__, fx__, tol__, del__
+        elif ared < 0.0:  # norm increased: smaller step
+            st.new_del = snrm * 0.5
+            ginfo = 2
+        elif ared / pred < 0.75:  # step ok: try a smaller one
+            x__, fx__, tol__ = st.new_x.clone(), st.new_fx.clone(), st.new_tol
+            del__ = snrm if ared / pred > 0.1 else snrm * 0.5
+            st.new_del = snrm * 0.7
+            ginfo = 2
+        elif snrm < st.new_del * 0.9:  # full Newton step taken
+            st.new_del = min(mxdl_, snrm * 2.0)
+        elif st.new_del < mxdl_ * 0.9:  # good step: try a larger one
+            x__, fx__, tol__, del__ = st.new_x.clone(), st.new_fx.clone(), st.new_tol, st.new_del
+            st.new_del = min(mxdl_, snrm * 2.0)
+            ginfo = 2
+        if ginfo == 2:
+            continue
+        st.new_nits += 1
+        hist.append((st.new_nits, st.new_gits, st.new_tol, st.new_del))
+        if sub:
+            sub()
+        x_, fx_, tol_ = st.new_x.clone(), st.new_fx.clone(), st.new_tol
+        tol__ = 1e99
+        if st.new_tol < tol:
+            return result(0)
+        if st.new_nits == nits:
+            return result(2)
+
+
+# ---------------------------------------------------------------------------
+# the orbit module (newton.f90)
+# ---------------------------------------------------------------------------
+class Orbit(NewtonState):
+    """newton.f90's orbit module for one pipe: ms = len(ndts) shooting
+    points, ndts[p] timesteps from point p to p+1, shifts[p] = (theta shift,
+    z shift, period) as read from shifts.in.  All vectors are float64 CUDA
+    tensors of ms*n entries, n = 8 + 6*N*H.  The pipe's work is moved onto a
+    stream of its own that the vector arithmetic shares."""
+
+    def __init__(self, pipe: Pipe, ndts, shifts, T_fixed: bool = False, epsJ: float = 1e-6):
+        if not torch.cuda.is_available():
+            raise PipeflowError(L.PF_ERR_NODEVICE, "Orbit: no CUDA device")
+        self.pipe = pipe
+        self.lib = pipe.lib
+        self.ctx = pipe.ctx
+        dev = pipe.device if pipe.device >= 0 else torch.cuda.current_device()
+        self.dev = torch.device("cuda", dev)
+        self.stream = torch.cuda.Stream(device=self.dev)
+        _check(self.lib.pf_ctx_set_stream(self.ctx, C.c_void_p(self.stream.cuda_stream)))
+        nn = C.c_longlong()
+        _check(self.lib.pf_orbit_vec_len(self.ctx, C.byref(nn)))
+        self.n = nn.value
+        self.ndts = [int(d) for d in ndts]
+        self.ms = len(self.ndts)
+        if self.ms < 1 or len(shifts) != self.ms:
+            raise PipeflowError(L.PF_ERR_ARG, "Orbit: one (theta shift, z shift, period) per shooting point")
+        self.T_fixed = T_fixed
+        self.epsJ = epsJ
+        self.scaleU = np.ones(3)
+        self.scaleT = 1.0
+        with torch.cuda.stream(self.stream):
+            self.new_x = torch.zeros(self.ms * self.n, dtype=torch.float64, device=self.dev)
+            hdr = torch.tensor(np.asarray(shifts, dtype=np.float64).reshape(self.ms, 3), device=self.dev)
+            self.new_x.view(self.ms, self.n)[:, :3] = hdr
+            self.new_fx = torch.zeros_like(self.new_x)
+        self.history = []
+
+    # -- vector maps -------------------------------------------------------
+    def _part(self, v: torch.Tensor, p: int) -> torch.Tensor:
+        return v[p * self.n:(p + 1) * self.n]
+
+    def set_scales(self, scaleU, scaleT: float) -> None:
+        self.scaleU = np.asarray(scaleU, dtype=np.float64).copy()
+        self.scaleT = float(scaleT)
+        _check(self.lib.pf_orbit_set_scales(self.ctx, self.scaleU.ctypes.data_as(L.DP), self.scaleT))
+
+    def rtz2vec(self, v: torch.Tensor) -> None:
+        """vel_ur, vel_ut, vel_uz -> v[8:n] (newton.f90:567-602)."""
+        _check(self.lib.pf_orbit_rtz2vec(self.ctx, C.c_void_p(_ptr(v))))
+
+    def vec2rtz(self, v: torch.Tensor) -> None:
+        """v -> vel_ur, vel_ut, vel_uz (newton.f90:608-643)."""
+        _check(self.lib.pf_orbit_vec2rtz(self.ctx, C.c_void_p(_ptr(v))))
+
+    def dotprod(self, n_: int, a: torch.Tensor, b: torch.Tensor) -> float:
+        """newton.f90:652-672: n_ = -1 leaves out the 8 header entries."""
+        out = C.c_double()
+        _check(self.lib.pf_orbit_dotprod(self.ctx, int(n_), C.c_void_p(_ptr(a)), C.c_void_p(_ptr(b)),
+                                         C.byref(out)))
+        return out.value
+
+    def dotprod_ms(self, n_: int, a: torch.Tensor, b: torch.Tensor) -> float:
+        """newton.f90:678-689."""
+        return sum(self.dotprod(n_, self._part(a, p), self._part(b, p)) for p in range(self.ms))
+
+    def getshiftdir(self, i: int, x: torch.Tensor) -> torch.Tensor:
+        """newton.f90:533-561: direction of a theta (i=1) or z (i=2) shift."""
+        with torch.cuda.stream(self.stream):
+            s = torch.zeros(self.n, dtype=torch.float64, device=self.dev)
+        _check(self.lib.pf_orbit_shiftdir(self.ctx, int(i), C.c_void_p(_ptr(x)), C.c_void_p(_ptr(s))))
+        return s
+
+    def steporbit(self, ndts: int, x: torch.Tensor, y: torch.Tensor) -> None:
+        """newton.f90:721-831 (no continuation, no output): y[8:] = the
+        state ndts steps from x, shifted back for ndts != 1."""
+        s = self.lib.pf_orbit_step(self.ctx, int(ndts), C.c_void_p(_ptr(x)), C.c_void_p(_ptr(y)))
+        if s not in (L.PF_OK, L.PF_ERR_CONVERGE):
+            _check(s)
+
+    # -- set-up (newton.f90:272-394) ----------------------------------------
+    def get_scales(self) -> None:
+        """newton.f90:272-305 from the pipe's current state: scaleU from the
+        energies of ur, ut and of uz without and with its mean mode, scaleT
+        from the first period and the size of the state vector."""
+        p = self.pipe
+        Er = p.var_coll_norm(p.vel_ur)[0]
+        Et = p.var_coll_norm(p.vel_ut)[0]
+        Ez = p.var_coll_norm(p.vel_uz)[0]
+        c1 = p.coll()
+        p.var_coll_copy(p.vel_uz, c1)
+        re, im = c1.download()
+        re[:, 0] = 0.0
+        c1.upload(re, im)
+        Ez00 = p.var_coll_norm(c1)[0]
+        Ez00 = Ez - Ez00
+        Ez = Ez - Ez00
+        self.set_scales([math.sqrt(0.2 * Ez00 / Er), math.sqrt(0.2 * Ez00 / Et), math.sqrt(0.5 * Ez00 / Ez)],
+                        1.0)
+        x0 = self._part(self.new_x, 0)
+        self.rtz2vec(x0)
+        d = self.dotprod(-1, x0, x0)
+        with torch.cuda.stream(self.stream):
+            scaleT = float(x0[2].item()) / math.sqrt(d)
+            self.new_x.view(self.ms, self.n)[:, :3] /= scaleT
+        self.set_scales(self.scaleU, scaleT)
+
+    def load_ms_states(self) -> None:
+        """newton.f90:311-350 without state files: shooting point p >= 1
+        is the state ndts[p-1] steps on from point p-1; point 0 is the
+        pipe's current state."""
+        self.rtz2vec(self._part(self.new_x, 0))
+        for p in range(1, self.ms):
+            x = self._part(self.new_x, p - 1).clone()
+            with torch.cuda.stream(self.stream):
+                y = torch.zeros(self.n, dtype=torch.float64, device=self.dev)
+            self.steporbit(self.ndts[p - 1], x, y)
+            with torch.cuda.stream(self.stream):
+                self._part(self.new_x, p)[8:] = y[8:]
+
+    def search_sz(self) -> None:
+        """newton.f90:356-394: for every shooting point whose shifts are
+        (0, -1), the z shift in [0, 2 pi/alpha) on a 0.01 grid that brings
+        the end state closest to the next point."""
+        p_ = self.pipe
+        n = self.n
+        for p1 in range(self.ms):
+            p = (p1 + 1) % self.ms
+            hdr = self._part(self.new_x, p1)[:2].cpu().numpy() * self.scaleT
+            st, sz = float(hdr[0]), float(hdr[1])
+            if abs(st) > 1e-8 or abs(sz + 1.0) > 1e-8:
+                continue
+            with torch.cuda.stream(self.stream):
+                x = self._part(self.new_x, p).clone()
+                y = self._part(self.new_x, p1).clone()
+                y[1] = 0.0
+            self.steporbit(self.ndts[p1], y, y)
+            self.vec2rtz(y)
+            r, t, z = p_.coll(), p_.coll(), p_.coll()
+            for i, c in enumerate((r, t, z)):
+                p_.var_coll_copy(p_.vel_field(i), c)
+            d1 = 1e99
+            sz = 0.0
+            sz_ = 0.0
+            alpha = p_.cfg.alpha
+            while sz < 2.0 * math.pi / alpha:
+                for i, c in enumerate((r, t, z)):
+                    p_.var_coll_shift(0.0, -sz, c, p_.vel_field(i))
+                self.rtz2vec(y)
+                with torch.cuda.stream(self.stream):
+                    dlt = y - x
+                d2 = self.dotprod(-1, dlt, dlt)
+                if d2 < d1:
+                    sz_ = sz
+                    d1 = d2
+                sz = sz + 0.01
+            with torch.cuda.stream(self.stream):
+                self.new_x[p1 * n + 1] = sz_ / self.scaleT
+
+    # -- the Newton operators (newton.f90:399-475, 837-860) -------------------
+    def getrhs(self, x: torch.Tensor) -> torch.Tensor:
+        """newton.f90:399-419: y = F(x) - x, header entries 0."""
+        n, ms = self.n, self.ms
+        with torch.cuda.stream(self.stream):
+            y_ = torch.zeros(n * ms, dtype=torch.float64, device=self.dev)
+        for p in range(ms):
+            p1 = (p + 1) % ms
+            self.steporbit(self.ndts[p], self._part(x, p), self._part(y_, p1))
+        with torch.cuda.stream(self.stream):
+            y = y_ - x
+            y.view(ms, n)[:, :8] = 0.0
+        return y
+
+    def multJ(self, x: torch.Tensor) -> torch.Tensor:
+        """newton.f90:425-465 (no continuation): finite-difference Jacobian
+        times x, with the constraint rows (no update along the shifts or
+        the trajectory; fixed period if T_fixed)."""
+        n, ms = self.n, self.ms
+        eps = math.sqrt(self.dotprod_ms(1, x, x))
+        if eps == 0.0:
+            raise PipeflowError(L.PF_ERR_ARG, "multJ: eps=0 (1)")
+        eps = self.epsJ * math.sqrt(self.dotprod_ms(1, self.new_x, self.new_x)) / eps
+        if eps == 0.0:
+            raise PipeflowError(L.PF_ERR_ARG, "multJ: eps=0 (2)")
+        with torch.cuda.stream(self.stream):
+            y = self.new_x + eps * x
+        s = self.getrhs(y)
+        with torch.cuda.stream(self.stream):
+            y = (s - self.new_fx) / eps
+        cfg = self.pipe.cfg
+        for p in range(ms):
+            xp = self._part(x, p)
+            nx = self._part(self.new_x, p)
+            vals = [0.0, 0.0, 0.0]
+            s = self.getshiftdir(1, nx)
+            vals[0] = self.dotprod(-1, s, xp)
+            s = self.getshiftdir(2, nx)
+            vals[1] = self.dotprod(-1, s, xp)
+            with torch.cuda.stream(self.stream):
+                s = torch.zeros(n, dtype=torch.float64, device=self.dev)
+            self.steporbit(1, nx, s)
+            dt = self.pipe.tim.dt
+            with torch.cuda.stream(self.stream):
+                s = (s - nx) / dt
+            vals[2] = self.dotprod(-1, s, xp)
+            if cfg.mirrorsym or cfg.shiftrefl or self.T_fixed:
+                xh = xp[:3].cpu().numpy()
+                if cfg.mirrorsym or cfg.shiftrefl:
+                    vals[0] = float(xh[0])
+                if self.T_fixed:
+                    vals[2] = float(xh[2])
+            with torch.cuda.stream(self.stream):
+                y[p * n:p * n + 3] = torch.tensor(vals, dtype=torch.float64, device=self.dev)
+        return y
+
+    def multA(self, x: torch.Tensor, y0: torch.Tensor, epsA: float) -> torch.Tensor:
+        """newton.f90:837-860: the linearised time-T map about new_x applied
+        to x (for the Arnoldi eigenvalue step), y0 = F(new_x)."""
+        n = self.n
+        with torch.cuda.stream(self.stream):
+            y = x.clone()
+        for p in range(self.ms):
+            nx = self._part(self.new_x, p)
+            eps = math.sqrt(self.dotprod(-1, y, y))
+            if eps == 0.0:
+                raise PipeflowError(L.PF_ERR_ARG, "multA: eps=0 (1)")
+            eps = epsA * math.sqrt(self.dotprod(-1, nx, nx)) / eps
+            if eps == 0.0:
+                raise PipeflowError(L.PF_ERR_ARG, "multA: eps=0 (2)")
+            with torch.cuda.stream(self.stream):
+                y = nx + eps * y
+                y[:8] = nx[:8]
+            self.steporbit(self.ndts[p], y, y)
+            with torch.cuda.stream(self.stream):
+                y = (y - self._part(y0, p)) / eps
+        return y
+
+    # -- the main program's search (newton.f90:102-128) -----------------------
+    def solve(self, m: int = 150, nits: int = 100, rel_err: float = 3e-6, delta: float = -1.0,
+              mndl: float = 1e-7, mxdl: float = 1e7, gtol: float = 1e-3) -> NewtonResult:
+        """newtonhook from new_x with the tolerances of newton_params.in
+        (rel_err, del, mndl, mxdl relative to |x|)."""
+        d = self.dotprod_ms(-1, self.new_x, self.new_x)
+        sd = math.sqrt(d)
+        tol = rel_err * sd
+
+        def f(v):
+            return self.getrhs(v)
+
+        def dp(a, b):
+            return self.dotprod_ms(1, a, b)
+
+        def sub():
+            nx = math.sqrt(self.dotprod_ms(-1, self.new_x, self.new_x))
+            hdr = self.new_x.view(self.ms, self.n)[:, :3].cpu().numpy() * self.scaleT
+            self.history.append(dict(nits=self.new_nits, gits=self.new_gits, tol=self.new_tol,
+                                     delta=self.new_del, rel=self.new_tol / nx, norm_x=nx,
+                                     shifts=hdr.tolist()))
+
+        with torch.cuda.stream(self.stream):
+            res = newtonhook(f, self.multJ, dp, self.new_x, m, gtol, tol, delta * sd, mndl * sd, mxdl * sd, nits,
+                             state=self, sub=sub)
+        self.stream.synchronize()
+        return res
+
+    def close(self) -> None:
+        """Give the pipe back its own stream."""
+        if self.ctx:
+            self.stream.synchronize()
+            _check(self.lib.pf_ctx_set_stream(self.ctx, None))
+            self.ctx = None
