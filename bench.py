@@ -389,24 +389,34 @@ def run_batched(args, torch, P, dist, world, rank, local):
     ms = ev0.elapsed_time(ev1)
     dom_ms, dom_n = batch.prof_read()[dom]
     batch.prof_enable(False)
-    # end to end through the C ABI: every pipe's state from pinned host
-    # memory in, one batch step, every state back out
-    host = []
-    for p in batch.pipes:
-        bufs = [torch.empty((p.H, p.N), dtype=torch.float64, pin_memory=True) for _ in range(6)]
-        ptrs = [P.api.C.cast(t.data_ptr(), P._lib.DP) for t in bufs]
+    # end to end through the C ABI: every step uploads a block with every
+    # pipe's state from pinned host memory, steps, and downloads the stepped
+    # states; the upload of the next block and the download of the last one
+    # run on copy streams while the step in between computes
+    nd = batch.io_bytes() // 8
+    hin = [torch.empty(nd, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    hout = [torch.empty(nd, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    off = 0
+    for p in batch.pipes:  # the block from the pipes' current states
+        n = p.N * p.H
+        ptrs = [P.api.C.cast(hin[0].data_ptr() + (off + k * n) * 8, P._lib.DP) for k in range(6)]
         P.api._check(p.lib.pf_vel_get_state(p.ctx, *ptrs))
-        host.append((bufs, ptrs))
+        off += 6 * n
+    hin[1].copy_(hin[0])
+    batch.put_states(0, hin[0])  # first use: allocates the device staging
+    batch.step_io(0, 1)
+    batch.get_states(0, hout[0])
+    batch.io_sync()
     ne = max(1, min(args.e2e_steps, args.steps))
     e0, e1 = dev_timer(torch, master)
     e0.record(master)
-    for _ in range(ne):
-        for p, (_, ptrs) in zip(batch.pipes, host):  # queued on each pipe's stream
-            P.api._check(p.lib.pf_vel_set_state(p.ctx, *ptrs))
-        batch.step(1)  # waits for the uploads on the device, returns after the step
-        for p, (_, ptrs) in zip(batch.pipes, host):
-            P.api._check(p.lib.pf_vel_get_state_async(p.ctx, *ptrs))
-        batch.sync()
+    batch.put_states(0, hin[0])
+    for s in range(ne):
+        if s + 1 < ne:
+            batch.put_states((s + 1) % 2, hin[(s + 1) % 2])
+        batch.step_io(s % 2, 1)
+        batch.get_states(s % 2, hout[s % 2])
+    batch.io_sync()
     e1.record(master)
     master.synchronize()
     e2e_ms = e0.elapsed_time(e1)
@@ -454,6 +464,8 @@ def run_batched(args, torch, P, dist, world, rank, local):
                                    "dominant_avg_launch_us": r["dom_ms"] * 1e3 / max(r["dom_n"], 1),
                                    **r["extra"]}
     return dict(ms=ms, e2e_ms=e2e_ms, ne=ne, count=args.pipes, launches=launches, clk=clk.summary(),
+                e2e_path="pf_batch_put_states / pf_batch_step_io / pf_batch_get_states: one pinned state block "
+                         "in and one out per step, copies on their own streams overlapping the step between",
                 extra=extra, dom=dom, dom_ms=dom_ms, dom_n=dom_n, per_launch=per_launch, h2d=io, d2h=io,
                 dtype="mixed: f32 transforms, f64 solves", config=config_of(args))
 
@@ -548,7 +560,8 @@ def main():
                          "traffic": read_traffic(r["dom"], args.workload)},
             "gpu_launches": r["launches"],
             "e2e": {"value": e2e_value, "unit": "timesteps/s", "steps": r["ne"],
-                    "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+                    "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
+                    "path": r.get("e2e_path", "")},
             "clocks": r["clk"],
         }
         if args.workload == "batched":

@@ -283,6 +283,33 @@ int pf_batch_step(pf_batch *b, int nsteps, int orbit, long long *corr_passes);
 int pf_batch_sync(pf_batch *b);
 /* The cudaStream_t the batch's graphs are launched on (for event timing). */
 int pf_batch_stream(pf_batch *b, void **stream);
+/* Pipelined state I/O of a whole batch.  No single reference routine: the
+ * host side of io.f90's state access (what pf_vel_set_state and
+ * pf_vel_get_state do per pipe), for every pipe at once and overlapped with
+ * stepping.  A state block holds every pipe's state in batch order; pipe i
+ * takes 6*N_i*H_i doubles: ur Re, ur Im, ut Re, ut Im, uz Re, uz Im, each
+ * H_i x N_i with the radial index fastest (%Re(n,nh)).  There are two input
+ * and two output slots on the device and one copy stream per direction:
+ *   put_states(s+1); step_io(s); get_states(s)
+ * with s alternating 0, 1 uploads the next block and downloads the last one
+ * while the step in between computes.  The first use allocates four blocks
+ * of device staging.  Host blocks should be page-locked for the copies to
+ * overlap.
+ * pf_batch_io_bytes: bytes of one state block for the current membership.
+ * pf_batch_put_states: queue the upload of `host` into input slot `slot`;
+ *   the host block may change once a pf_batch_step_io(slot, nsteps >= 1)
+ *   has returned, or after pf_batch_io_sync.
+ * pf_batch_step_io: every pipe's velocity from input slot `slot`, nsteps
+ *   steps as pf_batch_step, then the states into output slot `slot`;
+ *   PF_ERR_STATE if nothing was put into the slot since its last use.
+ * pf_batch_get_states: queue the download of output slot `slot` into `host`;
+ *   complete after pf_batch_io_wait(slot) or pf_batch_io_sync. */
+int pf_batch_io_bytes(pf_batch *b, unsigned long long *bytes);
+int pf_batch_put_states(pf_batch *b, int slot, const double *host);
+int pf_batch_step_io(pf_batch *b, int slot, int nsteps, int orbit, long long *corr_passes);
+int pf_batch_get_states(pf_batch *b, int slot, double *host);
+int pf_batch_io_wait(pf_batch *b, int slot);
+int pf_batch_io_sync(pf_batch *b);
 /* Kernel-category event timing for every pipe (see pf_prof_enable), and the
  * totals summed over the pipes.  Kernel spans of different pipes overlap in
  * time, so per-launch durations here include the sharing of the GPU. */

@@ -44,6 +44,7 @@ __global__ void k_batch_scalars(DevScalars *const *__restrict__ src, DevScalars 
     if (i < n) dst[i] = *src[i];
 }
 
+struct BatchIO;
 struct pf_batch {
     int n;
     std::vector<pf_ctx *> pipes;
@@ -81,7 +82,9 @@ struct pf_batch {
     pf_stage_prof sprof;             // stage timing of the batched launches
     std::vector<pf_stage_prof::Open> sev[2][2];
     unsigned long long launches;     // batched kernels launched (not per pipe)
+    struct BatchIO *io;              // pipelined state I/O (made on first use)
 };
+static void batch_io_free(pf_batch *b);
 
 static void staged_free(pf_batch *b) {
     pf_nl_batch_free(b->nlb);
@@ -130,6 +133,7 @@ static void batch_graphs_reset(pf_batch *b) {
 
 static void batch_free(pf_batch *b) {
     batch_graphs_reset(b);
+    batch_io_free(b);
     for (cudaEvent_t e : b->join) cudaEventDestroy(e);
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->master) cudaStreamDestroy(b->master);
@@ -664,5 +668,255 @@ extern "C" int pf_batch_staged(pf_batch *b, int *staged) {
 extern "C" int pf_batch_stream(pf_batch *b, void **stream) {
     PF_ARG(b && stream, "pf_batch_stream: bad argument");
     *stream = (void *)b->master;
+    return PF_OK;
+}
+
+// ------------------------------------------------------- pipelined state I/O
+// A state block holds the velocity states of every pipe of the batch, pipe
+// after pipe in batch order; pipe i takes 6*N_i*H_i doubles: ur Re, ur Im,
+// ut Re, ut Im, uz Re, uz Im, each H_i x N_i with the radial index fastest
+// (the layout of pf_vel_set_state's arrays, that of %Re(n,nh)).  Two input
+// and two output slots on the device, and one copy stream per direction, let
+// the upload of the next block and the download of the last one run while
+// the step in between computes.  No reference routine: the host side of
+// io.f90's state access for many pipes, overlapped with stepping.
+
+#define IO_MAX 64  // pipes per pack/unpack launch (kernel parameter space)
+
+struct IoPipe {
+    double2 *f[3];
+    long long off;  // doubles from the start of the block
+    int N, H, Hp;
+};
+struct IoArgs {
+    IoPipe p[IO_MAX];
+    int tile0[IO_MAX + 1];  // first 32x32 tile of each pipe (3 fields per pipe)
+    int n;
+};
+
+// block <-> device fields for up to IO_MAX pipes; one block per 32x32 tile
+// (radial points x modes) of one field, transposed through shared memory
+template <bool UNPACK>
+static __global__ void __launch_bounds__(256) k_batch_io(const __grid_constant__ IoArgs a, double *__restrict__ blk) {
+    __shared__ double2 tile[32][33];
+    const int b = blockIdx.x;
+    int p = 0;
+    while (p + 1 < a.n && a.tile0[p + 1] <= b) ++p;
+    const IoPipe &q = a.p[p];
+    const int N = q.N, H = q.H, Hp = q.Hp;
+    const int th = (H + 31) >> 5, tn = (N + 31) >> 5;
+    int t = b - a.tile0[p];
+    const int c = t / (th * tn);
+    t -= c * th * tn;
+    const int nh0 = (t % th) * 32, n0 = (t / th) * 32;
+    double *re = blk + q.off + (size_t)(2 * c) * H * N;
+    double *im = re + (size_t)H * N;
+    double2 *f = c == 0 ? q.f[0] : (c == 1 ? q.f[1] : q.f[2]);
+    if (UNPACK) {
+        for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+            const int nh = nh0 + i, n = n0 + threadIdx.x;
+            if (nh < H && n < N) {
+                const size_t at = (size_t)nh * N + n;
+                tile[i][threadIdx.x] = make_double2(re[at], im[at]);
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+            const int n = n0 + i, nh = nh0 + threadIdx.x;
+            if (n < N && nh < Hp) f[(size_t)n * Hp + nh] = nh < H ? tile[threadIdx.x][i] : make_double2(0.0, 0.0);
+        }
+    } else {
+        for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+            const int n = n0 + i, nh = nh0 + threadIdx.x;
+            if (n < N && nh < H) tile[threadIdx.x][i] = f[(size_t)n * Hp + nh];
+        }
+        __syncthreads();
+        for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+            const int nh = nh0 + i, n = n0 + threadIdx.x;
+            if (nh < H && n < N) {
+                const double2 v = tile[i][threadIdx.x];
+                const size_t at = (size_t)nh * N + n;
+                re[at] = v.x;
+                im[at] = v.y;
+            }
+        }
+    }
+}
+
+struct BatchIO {
+    size_t cap;  // doubles per slot
+    double *in[2], *out[2];
+    cudaStream_t up, down;
+    cudaEvent_t in_ready[2], in_free[2], out_ready[2], out_free[2];
+    bool filled[2];  // an upload into in[slot] has been queued
+};
+
+static void batch_io_free(pf_batch *b) {
+    BatchIO *io = b->io;
+    if (!io) return;
+    if (io->up) cudaStreamSynchronize(io->up);
+    if (io->down) cudaStreamSynchronize(io->down);
+    if (b->master) cudaStreamSynchronize(b->master);
+    for (int s = 0; s < 2; ++s) {
+        cudaFree(io->in[s]);
+        cudaFree(io->out[s]);
+        for (cudaEvent_t e : {io->in_ready[s], io->in_free[s], io->out_ready[s], io->out_free[s]})
+            if (e) cudaEventDestroy(e);
+    }
+    if (io->up) cudaStreamDestroy(io->up);
+    if (io->down) cudaStreamDestroy(io->down);
+    delete io;
+    b->io = nullptr;
+}
+
+// doubles of a state block for the current membership
+static size_t io_total(const pf_batch *b) {
+    size_t t = 0;
+    for (const pf_ctx *c : b->pipes) t += (size_t)6 * c->g.N * c->g.H;
+    return t;
+}
+
+// the I/O state with slots of at least `need` doubles
+static int io_ready(pf_batch *b, size_t need, BatchIO **out) {
+    if (!b->io) {
+        BatchIO *io = new BatchIO();
+        b->io = io;
+        PF_CUDA(cudaStreamCreateWithFlags(&io->up, cudaStreamNonBlocking));
+        PF_CUDA(cudaStreamCreateWithFlags(&io->down, cudaStreamNonBlocking));
+        for (int s = 0; s < 2; ++s)
+            for (cudaEvent_t *e : {&io->in_ready[s], &io->in_free[s], &io->out_ready[s], &io->out_free[s]})
+                PF_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    BatchIO *io = b->io;
+    if (need > io->cap) {
+        PF_CUDA(cudaStreamSynchronize(io->up));
+        PF_CUDA(cudaStreamSynchronize(io->down));
+        PF_CUDA(cudaStreamSynchronize(b->master));
+        for (int s = 0; s < 2; ++s) {
+            cudaFree(io->in[s]);
+            cudaFree(io->out[s]);
+            io->in[s] = io->out[s] = nullptr;
+            io->filled[s] = false;
+        }
+        io->cap = 0;
+        for (int s = 0; s < 2; ++s) {
+            if (cudaMalloc((void **)&io->in[s], need * sizeof(double)) != cudaSuccess ||
+                cudaMalloc((void **)&io->out[s], need * sizeof(double)) != cudaSuccess) {
+                cudaGetLastError();
+                pf_set_error("pf_batch state I/O: cannot allocate 4 x %zu bytes of staging", need * sizeof(double));
+                return PF_ERR_NOMEM;
+            }
+        }
+        io->cap = need;
+    }
+    *out = io;
+    return PF_OK;
+}
+
+// pack (UNPACK=false) or unpack every pipe's fields on the master stream
+static int io_launch(pf_batch *b, bool unpack, double *blk) {
+    long long off = 0;
+    for (int i0 = 0; i0 < b->n; i0 += IO_MAX) {
+        IoArgs a{};
+        a.n = std::min(IO_MAX, b->n - i0);
+        int tiles = 0;
+        for (int j = 0; j < a.n; ++j) {
+            pf_ctx *c = b->pipes[i0 + j];
+            IoPipe &q = a.p[j];
+            for (int f = 0; f < 3; ++f) q.f[f] = c->vel[f].d;
+            q.off = off;
+            q.N = c->g.N;
+            q.H = c->g.H;
+            q.Hp = c->g.Hp;
+            a.tile0[j] = tiles;
+            tiles += 3 * ((q.H + 31) / 32) * ((q.N + 31) / 32);
+            off += 6LL * q.N * q.H;
+        }
+        a.tile0[a.n] = tiles;
+        if (tiles == 0) continue;
+        if (unpack)
+            k_batch_io<true><<<tiles, dim3(32, 8), 0, b->master>>>(a, blk);
+        else
+            k_batch_io<false><<<tiles, dim3(32, 8), 0, b->master>>>(a, blk);
+        PF_CHECK_LAUNCH();
+        b->launches++;
+    }
+    return PF_OK;
+}
+
+extern "C" int pf_batch_io_bytes(pf_batch *b, unsigned long long *bytes) {
+    PF_ARG(b && bytes, "pf_batch_io_bytes: null argument");
+    *bytes = (unsigned long long)io_total(b) * sizeof(double);
+    return PF_OK;
+}
+
+extern "C" int pf_batch_put_states(pf_batch *b, int slot, const double *host) {
+    PF_ARG(b && host && (slot == 0 || slot == 1), "pf_batch_put_states: bad argument");
+    const size_t total = io_total(b);
+    BatchIO *io = nullptr;
+    PF_TRY(io_ready(b, std::max<size_t>(total, 1), &io));
+    PF_CUDA(cudaStreamWaitEvent(io->up, io->in_free[slot], 0));
+    PF_CUDA(cudaMemcpyAsync(io->in[slot], host, total * sizeof(double), cudaMemcpyHostToDevice, io->up));
+    PF_CUDA(cudaEventRecord(io->in_ready[slot], io->up));
+    io->filled[slot] = true;
+    return PF_OK;
+}
+
+extern "C" int pf_batch_step_io(pf_batch *b, int slot, int nsteps, int orbit, long long *corr_passes) {
+    PF_ARG(b && (slot == 0 || slot == 1) && nsteps >= 0, "pf_batch_step_io: bad argument");
+    const size_t total = io_total(b);
+    if (!b->io || b->io->cap < total || !b->io->filled[slot]) {
+        pf_set_error("pf_batch_step_io: no state block put into slot %d for this membership", slot);
+        return PF_ERR_STATE;
+    }
+    BatchIO *io = b->io;
+    // the block's upload, then every pipe's fields from it
+    PF_CUDA(cudaStreamWaitEvent(b->master, io->in_ready[slot], 0));
+    PF_TRY(io_launch(b, true, io->in[slot]));
+    PF_CUDA(cudaEventRecord(io->in_free[slot], b->master));
+    io->filled[slot] = false;
+    // steps that run per pipe on the pipes' own streams come after it
+    PF_CUDA(cudaEventRecord(b->fork, b->master));
+    for (pf_ctx *c : b->pipes) PF_CUDA(cudaStreamWaitEvent(c->stream, b->fork, 0));
+    const int s = pf_batch_step(b, nsteps, orbit, corr_passes);
+    if (s != PF_OK && s != PF_ERR_CONVERGE) return s;
+    for (int i = 0; i < b->n; ++i) {
+        PF_CUDA(cudaEventRecord(b->join[i], b->pipes[i]->stream));
+        PF_CUDA(cudaStreamWaitEvent(b->master, b->join[i], 0));
+    }
+    // the states into the output slot once its last download has finished
+    PF_CUDA(cudaStreamWaitEvent(b->master, io->out_free[slot], 0));
+    PF_TRY(io_launch(b, false, io->out[slot]));
+    PF_CUDA(cudaEventRecord(io->out_ready[slot], b->master));
+    return s;
+}
+
+extern "C" int pf_batch_get_states(pf_batch *b, int slot, double *host) {
+    PF_ARG(b && host && (slot == 0 || slot == 1), "pf_batch_get_states: bad argument");
+    const size_t total = io_total(b);
+    if (!b->io || b->io->cap < total) {
+        pf_set_error("pf_batch_get_states: no pf_batch_step_io has filled slot %d", slot);
+        return PF_ERR_STATE;
+    }
+    BatchIO *io = b->io;
+    PF_CUDA(cudaStreamWaitEvent(io->down, io->out_ready[slot], 0));
+    PF_CUDA(cudaMemcpyAsync(host, io->out[slot], total * sizeof(double), cudaMemcpyDeviceToHost, io->down));
+    PF_CUDA(cudaEventRecord(io->out_free[slot], io->down));
+    return PF_OK;
+}
+
+extern "C" int pf_batch_io_wait(pf_batch *b, int slot) {
+    PF_ARG(b && (slot == 0 || slot == 1), "pf_batch_io_wait: bad argument");
+    if (!b->io) return PF_OK;
+    PF_CUDA(cudaEventSynchronize(b->io->out_free[slot]));
+    return PF_OK;
+}
+
+extern "C" int pf_batch_io_sync(pf_batch *b) {
+    PF_ARG(b, "pf_batch_io_sync: null batch");
+    if (!b->io) return PF_OK;
+    PF_CUDA(cudaStreamSynchronize(b->io->up));
+    PF_CUDA(cudaStreamSynchronize(b->master));
+    PF_CUDA(cudaStreamSynchronize(b->io->down));
     return PF_OK;
 }

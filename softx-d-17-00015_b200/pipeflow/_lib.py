@@ -137,6 +137,12 @@ _SIGS = {
     "pf_batch_step": [P, I, I, C.POINTER(C.c_longlong)],
     "pf_batch_sync": [P],
     "pf_batch_stream": [P, PP],
+    "pf_batch_io_bytes": [P, C.POINTER(C.c_ulonglong)],
+    "pf_batch_put_states": [P, I, P],
+    "pf_batch_step_io": [P, I, I, I, C.POINTER(C.c_longlong)],
+    "pf_batch_get_states": [P, I, P],
+    "pf_batch_io_wait": [P, I],
+    "pf_batch_io_sync": [P],
     "pf_batch_prof_enable": [P, I],
     "pf_batch_prof_read": [P, I, DP, C.POINTER(C.c_ulonglong)],
     "pf_batch_launches": [P, C.POINTER(C.c_ulonglong)],

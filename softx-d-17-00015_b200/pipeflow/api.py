@@ -548,6 +548,39 @@ class Batch:
     def sync(self):
         _check(self.lib.pf_batch_sync(self.h))
 
+    # ---- pipelined state I/O (pf_batch_put_states / step_io / get_states)
+    def io_bytes(self) -> int:
+        """Bytes of one state block: every pipe's (ur, ut, uz) Re/Im, pipe
+        after pipe, each (H, N) with n fastest."""
+        b = C.c_ulonglong()
+        _check(self.lib.pf_batch_io_bytes(self.h, C.byref(b)))
+        return b.value
+
+    @staticmethod
+    def _host_ptr(buf) -> C.c_void_p:
+        if isinstance(buf, np.ndarray):
+            if buf.dtype != np.float64 or not buf.flags.c_contiguous:
+                raise PipeflowError(L.PF_ERR_ARG, "state block: contiguous float64 array required")
+            return C.c_void_p(buf.ctypes.data)
+        return C.c_void_p(buf.data_ptr())  # a torch tensor (page-locked for overlap)
+
+    def put_states(self, slot: int, host):
+        _check(self.lib.pf_batch_put_states(self.h, slot, self._host_ptr(host)))
+
+    def step_io(self, slot: int, nsteps: int = 1, orbit: bool = False) -> int:
+        n = C.c_longlong()
+        _check(self.lib.pf_batch_step_io(self.h, slot, nsteps, int(orbit), C.byref(n)))
+        return n.value
+
+    def get_states(self, slot: int, host):
+        _check(self.lib.pf_batch_get_states(self.h, slot, self._host_ptr(host)))
+
+    def io_wait(self, slot: int):
+        _check(self.lib.pf_batch_io_wait(self.h, slot))
+
+    def io_sync(self):
+        _check(self.lib.pf_batch_io_sync(self.h))
+
     def prof_enable(self, on=True):
         """on: True (all kernel categories), False, or a list of category names."""
         cats = Pipe.KERNEL_CATEGORIES

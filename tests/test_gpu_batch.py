@@ -219,3 +219,76 @@ def test_set_state_then_batch_step_is_ordered():
             assert np.array_equal(g, w)
         ap.close()
     batch.close()
+
+
+def _block(states):
+    """State block of pf_batch_put_states: per pipe ur Re, ur Im, ut Re, ut Im,
+    uz Re, uz Im, each (H, N) with n fastest."""
+    return np.concatenate([np.ascontiguousarray(x.T).ravel() for st in states for f in st for x in f])
+
+
+def _unblock(batch, blk):
+    out, off = [], 0
+    for p in batch.pipes:
+        n = p.N * p.H
+        a = [np.ascontiguousarray(blk[off + k * n:off + (k + 1) * n].reshape(p.H, p.N).T) for k in range(6)]
+        out.append([(a[0], a[1]), (a[2], a[3]), (a[4], a[5])])
+        off += 6 * n
+    return out
+
+
+@pytest.mark.parametrize("orbit", [False, True], ids=["main", "orbit"])
+def test_batch_pipelined_state_io(orbit):
+    """put_states / step_io / get_states with alternating slots: each output
+    block equals its input stepped alone through pf_timestep (bit for bit), a
+    zero-step pass returns its input unchanged, and a step without a block put
+    into its slot is refused."""
+    import pipeflow as P
+    cfgs = _cfgs()
+    batch = P.Batch(cfgs)
+    batch.matrices()
+    for i, bp in enumerate(batch.pipes):
+        _seed(bp, i)
+    batch.step(3, orbit=orbit)  # graphs captured for both parities
+    ins = []
+    for s in range(3):
+        sts = []
+        for i, c in enumerate(cfgs):
+            tmp = P.Pipe(c)
+            P.seeded_state(tmp, 700 + 10 * s + i, 1e-3)
+            sts.append(tmp.get_state())
+            tmp.close()
+        ins.append(_block(sts))
+    assert batch.io_bytes() == ins[0].nbytes
+    with pytest.raises(P.PipeflowError):
+        batch.step_io(1, 1)
+    back = np.empty_like(ins[0])
+    batch.put_states(0, ins[0])
+    batch.step_io(0, 0)
+    batch.get_states(0, back)
+    batch.io_wait(0)
+    assert np.array_equal(back, ins[0])
+    outs = [np.empty_like(ins[0]) for _ in range(3)]
+    batch.put_states(0, ins[0])
+    for s in range(3):
+        if s + 1 < 3:
+            batch.put_states((s + 1) % 2, ins[s + 1])
+        batch.step_io(s % 2, 2, orbit=orbit)
+        batch.get_states(s % 2, outs[s])
+    batch.io_sync()
+    for s in range(3):
+        want_all = _unblock(batch, ins[s])
+        got_all = _unblock(batch, outs[s])
+        for c, st, got in zip(cfgs, want_all, got_all):
+            ap = P.Pipe(c)
+            ap.vel_matrices()
+            ap.set_state(*st)
+            for _ in range(2):
+                if orbit:
+                    ap.steporbit(1)
+                else:
+                    ap.timestep()
+            for (gr, gi), (wr, wi) in zip(got, ap.get_state()):
+                assert np.array_equal(gr, wr) and np.array_equal(gi, wi)
+            ap.close()
+    batch.close()
