@@ -18,8 +18,10 @@ Entry points, named after the reference's routines:
                     mxdl=1e7, gtol=1e-3)     # the main program's call of newtonhook
 
 plus getrhs / multJ / multA / steporbit / dotprod / dotprod_ms / getshiftdir /
-rtz2vec / vec2rtz on device vectors.  Parameter continuation (Ctnu), the
-Arnoldi eigenvalue step and the output files are not included.
+rtz2vec / vec2rtz on device vectors, and get_eigen (newton.f90:868-979, the
+Arnoldi iteration of arnoldi.f on multA) for the Floquet spectrum of the
+converged orbit.  Parameter continuation (Ctnu) and the output files are not
+included.
 """
 from __future__ import annotations
 
@@ -242,6 +244,113 @@ def newtonhook(f, df, dp, x0, m, gtol, tol, delta, mndl, mxdl, nits, state: Newt
             return result(0)
         if st.new_nits == nits:
             return result(2)
+
+
+# ---------------------------------------------------------------------------
+# Arnoldi iteration (arnoldi.f) on device vectors
+# ---------------------------------------------------------------------------
+SMALL = 1e-80
+
+
+class Arnoldi:
+    """arnold (arnoldi.f:22-254): one call per new vector A.q_k.  The Krylov
+    basis q (kmax vectors) lives on the vectors' device, the Hessenberg
+    matrix h on the host; the eigenvalues of the k x k Hessenberg matrix come
+    from LAPACK's dgeev (balance, Hessenberg reduction, QR), which runs the
+    same dgebal / dgehrd / dhseqr sequence as the reference, and the
+    eigenvectors of the converged ones from the same decomposition (the
+    reference uses inverse iteration, dhsein; an eigenvector is defined up
+    to a scalar either way)."""
+
+    def __init__(self, n: int, kmax: int, ncgd: int, dp, tol: float, like: torch.Tensor):
+        self.n, self.kmax, self.ncgd, self.dp, self.tol = n, kmax, ncgd, dp, tol
+        self.q = torch.zeros((kmax, n), dtype=like.dtype, device=like.device)
+        self.h = np.zeros((kmax, kmax))
+        self.wr2 = np.zeros(ncgd)
+        self.wi2 = np.zeros(ncgd)
+        self.k = 0
+        self.b = None  # converged eigenvectors, columns as rows: (<= 2 ncgd, n)
+
+    def step(self, sv: torch.Tensor):
+        """Returns (ifail, sv): ifail -1 converged, 0 continue with sv <- A.sv,
+        1 reached kmax, 2 invariant subspace."""
+        k, h, q = self.k, self.h, self.q
+        if k >= self.kmax:
+            return 1, sv
+        q[k] = sv
+        for j in range(1, k + 1):  # modified Gram-Schmidt
+            h[j - 1, k - 1] = self.dp(q[k], q[j - 1])
+            q[k] -= h[j - 1, k - 1] * q[j - 1]
+        for j in range(1, k + 1):  # reorthogonalise
+            norm = self.dp(q[k], q[j - 1])
+            q[k] -= norm * q[j - 1]
+            h[j - 1, k - 1] += norm
+        norm = math.sqrt(self.dp(q[k], q[k]))
+        if norm < SMALL:
+            return 2, sv
+        q[k] /= norm
+        sv = q[k].clone()
+        ifail = 0
+        if k == 0:
+            h[:] = 0.0
+        else:
+            h[k, k - 1] = norm
+            if k >= self.ncgd:
+                ifail = self._eigen(k)
+        self.k = k + 1
+        return ifail, sv
+
+    def _eigen(self, k: int) -> int:
+        w, vr = scipy.linalg.eig(self.h[:k, :k], right=True)
+        wr, wi = w.real.copy(), w.imag.copy()
+        select = [False] * k
+        p = 0
+        for i in range(self.ncgd):  # largest magnitude first; compare with the last call's
+            norm, m = -1.0, 0
+            for j in range(k):
+                if not select[j]:
+                    nm = wr[j] * wr[j] + wi[j] * wi[j]
+                    if nm > norm:
+                        norm, m = nm, j
+            select[m] = True
+            if abs(wi[m]) > SMALL and m + 1 < k:
+                select[m + 1] = True
+            if math.hypot(wr[m] - self.wr2[i], wi[m] - self.wi2[i]) < self.tol:
+                p += 1
+            self.wr2[i], self.wi2[i] = wr[m], wi[m]
+        if p < self.ncgd:
+            return 0
+        # eigenvectors of h for the converged values, in wr2 order: one
+        # column for a real value, (Re, Im) for a complex pair
+        cols = []
+        for i in range(self.ncgd):
+            j = int(np.argmin(np.abs(w - complex(self.wr2[i], self.wi2[i]))))
+            v = vr[:, j]
+            v = v / np.max(np.abs(v.real) + np.abs(v.imag))  # dhsein's normalisation
+            cols.append(v.real)
+            if abs(self.wi2[i]) > SMALL:
+                cols.append(v.imag)
+        V = torch.as_tensor(np.array(cols), dtype=self.q.dtype).to(self.q.device)
+        self.b = V @ self.q[:k]
+        return -1
+
+
+def logeig(wr: np.ndarray, wi: np.ndarray, t: float):
+    """logeig (arnoldi.f:264-312): Floquet multipliers w = wr + i wi of the
+    period-t map to exponents sigma with w = exp(sigma t)."""
+    sr, si = np.empty_like(wr), np.empty_like(wi)
+    for i, (re, im) in enumerate(zip(wr, wi)):
+        if abs(re) < SMALL:
+            if abs(im) < SMALL:
+                raise PipeflowError(L.PF_ERR_ARG, f"logeig: zero multiplier {i + 1}")
+            th = 0.5 * math.pi if im > 0.0 else -0.5 * math.pi
+        elif re > 0.0:
+            th = math.atan(im / re)
+        else:
+            th = math.pi + math.atan(im / re) if im > 0.0 else -math.pi + math.atan(im / re)
+        sr[i] = math.log(math.sqrt(re * re + im * im)) / t
+        si[i] = th / t
+    return sr, si
 
 
 # ---------------------------------------------------------------------------
@@ -480,6 +589,79 @@ class Orbit(NewtonState):
             with torch.cuda.stream(self.stream):
                 y = (y - self._part(y0, p)) / eps
         return y
+
+    # -- Floquet analysis of the converged orbit (newton.f90:868-979) ---------
+    def get_eigen(self, m: int = 150, ncgd: int = 5, rel_err: float = 3e-6, gtol: float = 1e-3) -> dict:
+        """getEigen without the output files: Arnoldi on the linearised
+        period map about new_x (multA), started from new_x shifted by 0.3 of
+        the periods in theta and z with (1 - r^2) r^2 added to ur and ut of
+        modes (k,m) = (1,0) and (0,1).  Returns the Floquet multipliers, their
+        magnitude and angle, the Floquet exponents and the eigenvectors
+        scaled to the energy of the orbit (rows of a device tensor)."""
+        n, ms = self.n, self.ms
+        epsA = self.epsJ
+        rerr = min(rel_err, gtol)
+        t = float(self.new_x.view(ms, n)[:, 2].sum().item()) * self.scaleT
+        with torch.cuda.stream(self.stream):
+            y0 = torch.zeros_like(self.new_x)
+        for p in range(ms):
+            self.steporbit(self.ndts[p], self._part(self.new_x, p), self._part(y0, p))
+        pp = self.pipe
+        self.vec2rtz(self._part(self.new_x, 0))
+        st, sz = 0.3 * 2.0 * math.pi, 0.3 * 2.0 * math.pi / pp.cfg.alpha
+        for i in range(3):
+            pp.var_coll_shift(st, sz, pp.vel_field(i), pp.vel_field(i))
+        r2 = pp.mes_D()["r"] ** 2
+        prof = (1.0 - r2) * r2
+        for i in range(2):
+            f = pp.vel_field(i)
+            re, im = f.download()
+            for nh in (1, 2 * pp.K - 1):  # var_harmonic(1,0), var_harmonic(0,1)
+                if nh < pp.H:
+                    re[:, nh] = prof
+            f.upload(re, im)
+        pp.vel_imposesym()
+        with torch.cuda.stream(self.stream):
+            sv = torch.zeros(n, dtype=torch.float64, device=self.dev)
+        self.rtz2vec(sv)
+        ar = Arnoldi(n, m, ncgd, lambda a, b: self.dotprod(-1, a, b), rerr, sv)
+        status = "converged"
+        with torch.cuda.stream(self.stream):
+            while True:
+                sv[:8] = 0.0
+                ifail, sv = ar.step(sv)
+                if ifail == -1:
+                    break
+                if ifail == 0:
+                    sv = self.multA(sv, y0, epsA)
+                elif ifail == 1:
+                    status = "reached max iterations"
+                    break
+                else:
+                    raise PipeflowError(L.PF_ERR_CONVERGE, "getEigen: arnoldi error (invariant subspace)")
+        wr, wi = ar.wr2.copy(), ar.wi2.copy()
+        mag, ang = np.hypot(wr, wi), np.arctan2(wi, wr)
+        sr, si = logeig(wr, wi, t)
+        out = dict(its=ar.k, epsA=epsA, T=t, status=status, multipliers=(wr, wi), magnitude=mag, angle=ang,
+                   exponents=(sr, si), eigvecs=None)
+        if ar.b is not None:
+            # eigenvectors scaled to the energy of the orbit
+            def energy(v):
+                self.vec2rtz(v)
+                return sum(pp.var_coll_norm(pp.vel_field(c))[0] for c in range(3))
+            E0 = energy(self._part(self.new_x, 0))
+            b = ar.b
+            j = 0
+            for i in range(ncgd):
+                npart = 2 if wi[i] != 0.0 else 1
+                E = sum(energy(b[j + q]) for q in range(npart))
+                if E > 0.0:
+                    with torch.cuda.stream(self.stream):
+                        b[j:j + npart] *= math.sqrt(E0 / E)
+                j += npart
+            out["eigvecs"] = b
+        self.stream.synchronize()
+        return out
 
     # -- the main program's search (newton.f90:102-128) -----------------------
     def solve(self, m: int = 150, nits: int = 100, rel_err: float = 3e-6, delta: float = -1.0,

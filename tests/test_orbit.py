@@ -244,3 +244,93 @@ def test_device_multJ_and_short_newton_search():
     assert rg.tol < ro.history[0][2]  # the residual went down
     assert len(orb.history) == 3
     orb.close()
+
+
+def test_arnoldi_host_logic_finds_leading_eigenpairs():
+    """arnold (arnoldi.f) on a dense operator with known spectrum: the
+    converged values are the largest-magnitude eigenvalues, in that order,
+    and the returned vectors are eigenvectors (Re, Im columns for a pair)."""
+    from pipeflow.newton import Arnoldi, logeig
+    rng = np.random.default_rng(5)
+    n = 40
+    lam = np.concatenate([[0.95], [0.9 + 0.2j, 0.9 - 0.2j], rng.uniform(-0.5, 0.5, n - 3)])
+    # a real operator with these eigenvalues: 2x2 rotation-scaling block for the pair
+    D = np.zeros((n, n))
+    D[0, 0] = 0.95
+    D[1:3, 1:3] = [[0.9, 0.2], [-0.2, 0.9]]
+    for i in range(3, n):
+        D[i, i] = lam[i].real
+    X = rng.standard_normal((n, n))
+    A = X @ D @ np.linalg.inv(X)
+    At = torch.tensor(A)
+    ar = Arnoldi(n, 40, 2, lambda a, b: float(a @ b), 1e-10, torch.zeros(n, dtype=torch.float64))
+    sv = torch.tensor(rng.standard_normal(n))
+    while True:
+        ifail, sv = ar.step(sv)
+        if ifail != 0:
+            break
+        sv = At @ sv
+    assert ifail == -1
+    got = ar.wr2 + 1j * ar.wi2
+    assert abs(got[0] - 0.95) < 1e-9
+    assert abs(got[1] - (0.9 + 0.2j)) < 1e-9
+    b = ar.b.numpy()
+    assert b.shape == (3, n)
+    assert np.linalg.norm(A @ b[0] - 0.95 * b[0]) < 1e-8 * np.linalg.norm(b[0])
+    v = b[1] + 1j * b[2]
+    assert np.linalg.norm(A @ v - (0.9 + 0.2j) * v) < 1e-8 * np.linalg.norm(v)
+    sr, si = logeig(ar.wr2, ar.wi2, 2.0)
+    assert sr[1] == pytest.approx(math.log(abs(0.9 + 0.2j)) / 2.0, rel=1e-9)
+    assert si[1] == pytest.approx(math.atan2(0.2, 0.9) / 2.0, rel=1e-9)
+
+
+@pytest.mark.gpu
+def test_device_floquet_spectrum_matches_dense_linear_map():
+    """get_eigen (Arnoldi on multA, newton.f90:868-979) about a 1e-12-energy
+    state, i.e. about laminar flow to first order: the converged Floquet
+    multipliers of the 50-step map are eigenvalues of the 50th power of the
+    oracle's dense linearised one-step map (all modes, 6NH x 6NH), the
+    leading one the largest.  Re = 100 and T = 0.5 keep the leading
+    multipliers apart, so the reference's stopping rule (successive Ritz
+    values within min(rel_err, gtol)) stops on converged values."""
+    import pipeflow as P
+    from pipeflow.newton import Orbit
+    cfgd = dict(N=16, K=2, M=2, Re=100.0, alpha=1.0, dt=0.01)
+    o = oracle_pipe(cfgd)
+    o.vel_matrices()
+    N, H = o.N, o.H
+    ns = 6 * N * H
+    eps = 1e-8
+
+    def unpack(vec):
+        a = vec.reshape(3, 2, N, H)
+        return [O.Coll(a[c, 0].copy(), a[c, 1].copy()) for c in range(3)]
+
+    def pack(st):
+        return np.concatenate([np.concatenate([f.re.ravel(), f.im.ravel()]) for f in st])
+
+    J = np.empty((ns, ns))
+    for i in range(ns):
+        e = np.zeros(ns)
+        e[i] = eps
+        o.set_state(*unpack(e))
+        o.timestep(orbit=True)
+        J[:, i] = pack(o.state()) / eps
+    mu = np.linalg.eigvals(J) ** 50
+    g = device_pipe(cfgd)
+    g.vel_matrices()
+    P.seeded_state(g, 3, 1e-12)
+    orb = Orbit(g, [50], [(0.0, 0.0, 0.5)])
+    orb.set_scales([1.0, 1.0, 1.0], 1.0)
+    orb.rtz2vec(orb.new_x)
+    res = orb.get_eigen(m=80, ncgd=2)
+    assert res["status"] == "converged"
+    wr, wi = res["multipliers"]
+    lams = wr + 1j * wi
+    assert abs(lams[0] - mu[np.argmax(np.abs(mu))]) < 1e-6 * abs(lams[0])
+    for lam in lams[1:]:
+        assert np.min(np.abs(mu - lam)) < 1e-4 * abs(lam)
+    sr, _ = res["exponents"]
+    assert sr[0] == pytest.approx(math.log(abs(lams[0])) / 0.5, rel=1e-12)
+    assert res["eigvecs"] is not None
+    orb.close()
