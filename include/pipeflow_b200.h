@@ -260,6 +260,35 @@ int pf_orbit_step(pf_ctx *ctx, int ndts, const double *x, double *y);
 int pf_diag_energy(pf_ctx *ctx, double *E);
 int pf_diag_friction(pf_ctx *ctx, double *Ub, double *Uc, double *Ufr);
 
+/* ------------------------------------------------------------ state files */
+/* The netCDF-3 state files of io.f90 (state*.cdf.dat / state.cdf.in):
+ * dimensions r, H, ReIm; global attributes t, Re, alpha; variables r, dt,
+ * dtcor, dtcfl and Ur, Ut, Uz(ReIm, H, r) with attributes K, M, Mp.  Written
+ * and parsed without libnetcdf (the format is the published netCDF classic /
+ * 64-bit-offset layout).
+ * pf_io_save_state: io_save_state (io.f90:303-378) of the context's state,
+ *   mesh, t, dt, corr/CFL dt, Re and alpha to `path`.
+ * pf_io_load_state: io_load_state (io.f90:98-226) into the context: radial
+ *   interpolation (io_interp_wts/io_interp, io.f90:232-288) when the file's
+ *   mesh differs, K/M re-truncation with zero fill, t from the file if
+ *   flags has PF_IO_TIME_FROM_FILE (the reference's d_time < 0), dt from the
+ *   file for an adaptive-dt run (dt < 0) else the configured dt, and the
+ *   file's dtcor/dtcfl if present.  *changes (may be NULL) gets bit 1 if
+ *   interpolated, 2 if K, 4 if M, 8 if Mp differed.  New dt needs
+ *   pf_vel_matrices before stepping, as in the reference's initialise.
+ * pf_state_write / pf_state_read: the same without a context or a GPU, on
+ *   host arrays in pf_vel_set_state's layout (H x N, radial index fastest);
+ *   r is the N radial points written / to interpolate onto; scalars holds
+ *   t, Re, alpha, dt, dtcor, dtcfl (read: NaN where the file has none). */
+#define PF_IO_TIME_FROM_FILE 1
+int pf_io_save_state(pf_ctx *ctx, const char *path);
+int pf_io_load_state(pf_ctx *ctx, const char *path, int flags, int *changes);
+int pf_state_write(const char *path, int N, int K, int M, int Mp, const double *r, const double *ur_re,
+                   const double *ur_im, const double *ut_re, const double *ut_im, const double *uz_re,
+                   const double *uz_im, const double *scalars);
+int pf_state_read(const char *path, int N, int K, int M, int Mp, const double *r, double *ur_re, double *ur_im,
+                  double *ut_re, double *ut_im, double *uz_re, double *uz_im, double *scalars, int *changes);
+
 /* ----------------------------------------------------------------- batches */
 /* Many independent pipes of uneven (N, K, M, Re, alpha, dt) advanced together;
  * one timestep of the batch is a single CUDA graph.  Where every pipe fits

@@ -20,6 +20,7 @@ PF_ERR_CONVERGE = -6
 PF_ERR_NODEVICE = -7
 PF_PREC_FP64 = 0
 PF_PREC_MIXED = 1
+PF_IO_TIME_FROM_FILE = 1
 KL = 4
 
 
@@ -121,6 +122,10 @@ _SIGS = {
     "pf_vel_influence_download": [P, DP, DP],
     "pf_timestep": [P, IP],
     "pf_steporbit": [P, I],
+    "pf_io_save_state": [P, C.c_char_p],
+    "pf_io_load_state": [P, C.c_char_p, I, IP],
+    "pf_state_write": [C.c_char_p, I, I, I, I, DP, DP, DP, DP, DP, DP, DP, DP],
+    "pf_state_read": [C.c_char_p, I, I, I, I, DP, DP, DP, DP, DP, DP, DP, DP, IP],
     "pf_orbit_set_scales": [P, DP, D],
     "pf_orbit_vec_len": [P, C.POINTER(C.c_longlong)],
     "pf_orbit_rtz2vec": [P, P],

@@ -458,6 +458,18 @@ class Pipe:
     def steporbit(self, nsteps: int):
         _check(self.lib.pf_steporbit(self.ctx, nsteps))
 
+    # ---------------- io.f90 state files ----------------
+    def io_save_state(self, path):
+        """io_save_state (io.f90:303-378): this pipe's state to a netCDF file."""
+        from .statefile import io_save_state
+        io_save_state(self, path)
+
+    def io_load_state(self, path, time_from_file: bool = False) -> int:
+        """io_load_state (io.f90:98-226): interpolated and re-truncated onto
+        this pipe; returns the change bits (1 mesh, 2 K, 4 M, 8 Mp)."""
+        from .statefile import io_load_state
+        return io_load_state(self, path, time_from_file)
+
     def energy(self) -> float:
         E = C.c_double()
         _check(self.lib.pf_diag_energy(self.ctx, C.byref(E)))
