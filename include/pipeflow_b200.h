@@ -260,6 +260,31 @@ int pf_orbit_step(pf_ctx *ctx, int ndts, const double *x, double *y);
 int pf_diag_energy(pf_ctx *ctx, double *E);
 int pf_diag_friction(pf_ctx *ctx, double *Ub, double *Uc, double *Ufr);
 
+/* ------------------------------------------------------------ util hook */
+/* The plug-in hook of main.f90: var_null(2) after every evaluation of the
+ * nonlinear terms, var_null(1) once per step before the predictor
+ * (main.f90:23,30,38); pf_timestep calls it when a plug-in is set (and then
+ * runs eagerly, without its graphs; orbit steps, like newton.f90's
+ * steporbit, do not call it).  Built-in plug-ins, on the device:
+ *   PF_UTIL_CORIOLIS: params Ek0, phi -- Coriolis.f90:13-73 (Mp must be 1)
+ *   PF_UTIL_CARREAU_YASUDA: params rho, radius, mu_0, mu_inf, lam_CY, n_CY,
+ *     a_CY[, fc1] -- nonnewtonian.f90:32-246; sets one corrector pass per
+ *     step (tim_pcn = 1) as the reference does
+ * A host callback fn(ctx, flag, user) runs after the built-in at both
+ * flags, for plug-ins written against this ABI (adding to vel_Nr/Nt/Nz
+ * through pf_vel_coll and pf_var_coll_add).  pf_util runs the hook once, for
+ * drivers that step through the module calls themselves. */
+#define PF_UTIL_NONE            0
+#define PF_UTIL_CORIOLIS        1
+#define PF_UTIL_CARREAU_YASUDA  2
+typedef void (*pf_util_fn)(pf_ctx *ctx, int flag, void *user);
+int pf_util_set(pf_ctx *ctx, int kind, const double *params, int nparams);
+int pf_util_set_callback(pf_ctx *ctx, pf_util_fn fn, void *user);
+int pf_util(pf_ctx *ctx, int flag);
+/* nu at the wall (mean mode), min and max over the grid from the last
+ * Carreau-Yasuda evaluation (write_Re_nu, nonnewtonian.f90:302-318) */
+int pf_util_nu_stats(pf_ctx *ctx, double *nu_wall, double *nu_min, double *nu_max);
+
 /* ------------------------------------------------------------ state files */
 /* The netCDF-3 state files of io.f90 (state*.cdf.dat / state.cdf.in):
  * dimensions r, H, ReIm; global attributes t, Re, alpha; variables r, dt,

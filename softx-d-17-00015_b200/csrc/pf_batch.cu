@@ -273,7 +273,8 @@ extern "C" int pf_batch_matrices(pf_batch *b) {
 
 static bool batch_graphable(const pf_batch *b) {
     for (const pf_ctx *c : b->pipes)
-        if (!(c->cfg.dt > 0.0 && c->matrices_ready && pf_nl_fused_supported(c) && pf_fused_step_ok(c)))
+        if (!(c->cfg.dt > 0.0 && c->matrices_ready && pf_nl_fused_supported(c) && pf_fused_step_ok(c)) ||
+            pf_util_active(c))
             return false;
     return true;
 }

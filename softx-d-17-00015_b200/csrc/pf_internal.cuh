@@ -168,6 +168,17 @@ struct pf_ctx {
     double orbit_scaleU[3], orbit_scaleT;
     bool orbit_set;
     double *orbit_red;   // ORBIT_DOT_BLOCKS + 1 doubles
+    // util plug-in (var_null hook of main.f90): built-in kind, its
+    // parameters, device scratch, host callback, nu diagnostics
+    int util_kind;
+    double util_par[8];
+    double *util_phys;
+    int util_nphys;
+    double *util_coll;
+    int util_ncoll;
+    pf_util_fn util_cb;
+    void *util_user;
+    double *util_diag_d;
     unsigned long long *cflmax;  // 3*N CFL maxima of the last fused transform
     bool cfl_fused;              // cflmax is current (else use vel_r/t/z)
     int *anypiv;         // per LU set: 1 if dgbtf2 swapped any row
@@ -299,6 +310,8 @@ int pf_launch_phys2coll(pf_ctx *ctx, int ncomp, const double *const *src,
 int pf_launch_maxtstep(pf_ctx *ctx, double *dt3);
 int pf_norm_host(pf_ctx *ctx, const double2 *a, double *E, double *Ek, double *Em);
 bool pf_nl_fused_supported(const pf_ctx *ctx);
+bool pf_util_active(const pf_ctx *ctx);
+int pf_util_run(pf_ctx *ctx, int flag);
 
 // Batched launches: one launch per stage over the tiles of many pipes.
 // Stage timing of such launches (event pairs on the launching stream, made

@@ -264,7 +264,18 @@ static int replay(pf_ctx *ctx, int slot, cudaGraphExec_t g, unsigned long long n
 }
 
 static bool graphs_ok(const pf_ctx *ctx) {
-    return ctx->use_graphs && ctx->cfg.dt > 0.0 && pf_nl_fused_supported(ctx) && fused_step_ok(ctx);
+    return ctx->use_graphs && ctx->cfg.dt > 0.0 && pf_nl_fused_supported(ctx) && fused_step_ok(ctx) &&
+           !pf_util_active(ctx);
+}
+
+// vel_transform + vel_nonlinear + var_null(2) of the main loop (main.f90:21-23,
+// 36-38): with a plug-in the physical fields vel_r .. vel_curlz are made, as
+// the plug-ins read them
+static int main_nonlinear(pf_ctx *ctx) {
+    if (!pf_util_active(ctx)) return transform_nonlinear(ctx);
+    PF_TRY(pf_vel_transform(ctx));
+    PF_TRY(pf_vel_nonlinear(ctx));
+    return pf_util_run(ctx, 2);
 }
 
 // main.f90:20-44.  With a fixed dt and the fused kernels, the pass through
@@ -311,16 +322,17 @@ extern "C" int pf_timestep(pf_ctx *ctx, int *ncorr) {
         }
     } else {
         PF_TRY(pf_vel_imposesym(ctx));
-        PF_TRY(transform_nonlinear(ctx));
+        PF_TRY(main_nonlinear(ctx));
         if (ctx->cfg.dt < 0.0) {
             PF_TRY(pf_vel_maxtstep(ctx));
             PF_TRY(pf_tim_new_tstep(ctx));
             if (ctx->tim.new_dt) PF_TRY(pf_vel_matrices_impl(ctx));
         }
+        if (pf_util_active(ctx)) PF_TRY(pf_util_run(ctx, 1));
         PF_TRY(pf_vel_predictor(ctx));
         ctx->tim.it = 1;
         while (ctx->tim.it != 0) {
-            PF_TRY(transform_nonlinear(ctx));
+            PF_TRY(main_nonlinear(ctx));
             PF_TRY(pf_vel_corrector(ctx));
             const int s = pf_tim_check_cgce(ctx);
             if (s != PF_OK) status = s;

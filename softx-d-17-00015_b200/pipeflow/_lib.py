@@ -21,6 +21,10 @@ PF_ERR_NODEVICE = -7
 PF_PREC_FP64 = 0
 PF_PREC_MIXED = 1
 PF_IO_TIME_FROM_FILE = 1
+PF_UTIL_NONE = 0
+PF_UTIL_CORIOLIS = 1
+PF_UTIL_CARREAU_YASUDA = 2
+UTIL_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_void_p)
 KL = 4
 
 
@@ -122,6 +126,10 @@ _SIGS = {
     "pf_vel_influence_download": [P, DP, DP],
     "pf_timestep": [P, IP],
     "pf_steporbit": [P, I],
+    "pf_util_set": [P, I, DP, I],
+    "pf_util_set_callback": [P, P, P],
+    "pf_util": [P, I],
+    "pf_util_nu_stats": [P, DP, DP, DP],
     "pf_io_save_state": [P, C.c_char_p],
     "pf_io_load_state": [P, C.c_char_p, I, IP],
     "pf_state_write": [C.c_char_p, I, I, I, I, DP, DP, DP, DP, DP, DP, DP, DP],

@@ -458,6 +458,31 @@ class Pipe:
     def steporbit(self, nsteps: int):
         _check(self.lib.pf_steporbit(self.ctx, nsteps))
 
+    # ---------------- util plug-ins (main.f90's var_null hook) ----------------
+    def util_set(self, kind: int, params=()):
+        """Built-in plug-in: PF_UTIL_CORIOLIS (Ek0, phi) or PF_UTIL_CARREAU_YASUDA
+        (rho, radius, mu_0, mu_inf, lam_CY, n_CY, a_CY); PF_UTIL_NONE clears."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        _check(self.lib.pf_util_set(self.ctx, int(kind), _dp(p) if p.size else None, int(p.size)))
+
+    def util_set_callback(self, fn):
+        """fn(flag) runs at var_null(flag) inside pf_timestep (None clears)."""
+        if fn is None:
+            self._util_cb = None
+            _check(self.lib.pf_util_set_callback(self.ctx, None, None))
+            return
+        self._util_cb = L.UTIL_FN(lambda ctx, flag, user: fn(flag))
+        _check(self.lib.pf_util_set_callback(self.ctx, C.cast(self._util_cb, C.c_void_p), None))
+
+    def util(self, flag: int):
+        _check(self.lib.pf_util(self.ctx, int(flag)))
+
+    def util_nu_stats(self):
+        """(nu_wall, nu_min, nu_max) of the last Carreau-Yasuda evaluation."""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        _check(self.lib.pf_util_nu_stats(self.ctx, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
     # ---------------- io.f90 state files ----------------
     def io_save_state(self, path):
         """io_save_state (io.f90:303-378): this pipe's state to a netCDF file."""

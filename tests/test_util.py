@@ -1,0 +1,111 @@
+"""util plug-ins through main.f90's var_null hook (Coriolis.f90,
+nonnewtonian.f90) and the host callback.
+
+CPU: invariants of the oracle's restatements.  GPU: pf_timestep with each
+built-in plug-in against the oracle's main loop with the same plug-in, the
+Carreau-Yasuda viscosity statistics, and the order of the hook calls."""
+import numpy as np
+import pytest
+
+import pipeflow_oracle as O
+import util_oracle as UO
+from _util import SMALL, device_pipe, oracle_pipe, state_from_dev, state_to_dev
+
+CFG = dict(N=20, K=5, M=4, Mp=1, Re=2000.0, alpha=1.25, dt=0.01)
+CY = (1000.0, 0.01, 0.05, 0.0035, 3.3, 0.36, 2.0)  # rho, radius, mu_0, mu_inf, lam, n, a
+
+
+def _oracle(cfgd, seed=6):
+    o = oracle_pipe(cfgd)
+    o.vel_matrices()
+    st = O.seeded_state(o, seed, 1e-3)
+    o.set_state(*st)
+    return o, st
+
+
+def test_coriolis_about_the_pipe_axis_leaves_axial_terms():
+    """Omega along the pipe axis (phi = 0): Omega x u has no z component."""
+    o, _ = _oracle(CFG)
+    o.vel_imposesym()
+    o.vel_transform()
+    o.vel_nonlinear()
+    Nz = o.vel_Nz.copy()
+    Nr = o.vel_Nr.copy()
+    UO.coriolis(o, 0.5, 0.0)
+    assert np.array_equal(o.vel_Nz.re, Nz.re) or np.max(np.abs(o.vel_Nz.re - Nz.re)) < 1e-15
+    assert np.max(np.abs(o.vel_Nr.re - Nr.re)) > 1e-9
+
+
+def test_carreau_yasuda_newtonian_limit_adds_nothing():
+    """mu_inf = mu_0 makes nu = 1 everywhere: no extra stress."""
+    o, _ = _oracle(CFG)
+    o.vel_imposesym()
+    o.vel_transform()
+    o.vel_nonlinear()
+    N0 = [o.vel_Nr.copy(), o.vel_Nt.copy(), o.vel_Nz.copy()]
+    stats = UO.carreau_yasuda(o, 1000.0, 0.01, 0.05, 0.05, 3.3, 0.36, 2.0)
+    assert stats[1] == pytest.approx(1.0, abs=1e-15) and stats[2] == pytest.approx(1.0, abs=1e-15)
+    assert O.rel_l2([o.vel_Nr, o.vel_Nt, o.vel_Nz], N0) < 1e-10
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["coriolis", "carreau_yasuda"])
+def test_plugin_steps_match_oracle(kind):
+    import pipeflow as P
+    o, st = _oracle(CFG)
+    g = device_pipe(CFG)
+    g.vel_matrices()
+    state_to_dev(g, st)
+    if kind == "coriolis":
+        g.util_set(P._lib.PF_UTIL_CORIOLIS, (0.5, 0.3))
+        util = lambda op: UO.coriolis(op, 0.5, 0.3)  # noqa: E731
+    else:
+        g.util_set(P._lib.PF_UTIL_CARREAU_YASUDA, CY)
+        o.tim_pcn = 1  # nonnewtonian.f90:66-67
+        o.tim_it = 0
+        stats = []
+        util = lambda op: stats.append(UO.carreau_yasuda(op, *CY))  # noqa: E731
+    for _ in range(3):
+        no = UO.timestep_with_util(o, util)
+        ng = g.timestep()
+        assert no == ng
+    assert O.rel_l2(state_from_dev(g), o.state()) <= 1e-11
+    if kind == "carreau_yasuda":
+        wall, lo, hi = g.util_nu_stats()
+        assert wall == pytest.approx(stats[-1][0], rel=1e-11)
+        assert lo == pytest.approx(stats[-1][1], rel=1e-11) and hi == pytest.approx(stats[-1][2], rel=1e-11)
+        assert lo < hi <= 1.0
+
+
+@pytest.mark.gpu
+def test_callback_order_and_effect():
+    """The callback runs at var_null(2), var_null(1), var_null(2) for a step
+    with one corrector pass, and what it adds to vel_N changes the step as
+    the same addition does in the oracle's loop."""
+    import pipeflow as P
+    o, st = _oracle(CFG)
+    g = device_pipe(CFG)
+    g.vel_matrices()
+    state_to_dev(g, st)
+    flags = []
+    extra = P.Coll(g)
+    rng = np.random.default_rng(2)
+    add = O.Coll(1e-4 * rng.standard_normal((g.N, g.H)), np.zeros((g.N, g.H)))
+    add.re[:, 0] = 0.0
+    extra.upload(add.re, add.im)
+
+    def hook(flag):
+        flags.append(flag)
+        if flag == 2:
+            g.var_coll_add(extra, g.vel_Nz)
+
+    def util(op):
+        op.vel_Nz = O.Coll(op.vel_Nz.re + add.re, op.vel_Nz.im + add.im)
+
+    g.util_set_callback(hook)
+    no = UO.timestep_with_util(o, util)
+    ng = g.timestep()
+    assert flags[:3] == [2, 1, 2] and len(flags) == 2 + ng
+    assert no == ng
+    assert O.rel_l2(state_from_dev(g), o.state()) <= 1e-11
+    g.util_set_callback(None)
