@@ -262,26 +262,34 @@ def plain_sequential(P, torch, cfgs, seeds, steps=3):
     return total_steps / (total_ms / 1e3), total_ms / total_steps
 
 
-def mixed_error(P, d, seed, nsteps=100):
+def mixed_error(P, d, seed, nsteps=1000):
     """State rel-L2, kinetic-energy and friction errors of the mixed path
-    against FP64 on one pipe of the mix after nsteps."""
+    against FP64 on one pipe of the mix, after 1, 100 and 1000 steps (those
+    not beyond nsteps)."""
     g64 = P.Pipe(P.PipeConfig(**d))
     gm = P.Pipe(P.PipeConfig(**d, precision=P.PF_PREC_MIXED))
     for g in (g64, gm):
         g.vel_matrices()
         P.seeded_state(g, seed, 1e-3)
-        for _ in range(nsteps):
-            g.timestep()
-    num = den = 0.0
-    for (ar, ai), (br, bi) in zip(gm.get_state(), g64.get_state()):
-        num += float(np.sum((ar - br) ** 2 + (ai - bi) ** 2))
-        den += float(np.sum(br ** 2 + bi ** 2))
-    e64, em = g64.energy(), gm.energy()
-    f64, fm = g64.friction()[2], gm.friction()[2]
-    out = {"steps": nsteps, "pipe": d, "state_rel_l2": math.sqrt(num / den),
-           "energy_rel": abs(em - e64) / e64, "friction_rel": abs(fm - f64) / f64}
+    marks = [s for s in (1, 100, 1000) if s <= nsteps] or [nsteps]
+    rows = []
+    done = 0
+    for mark in marks:
+        for g in (g64, gm):
+            for _ in range(mark - done):
+                g.timestep()
+        done = mark
+        num = den = 0.0
+        for (ar, ai), (br, bi) in zip(gm.get_state(), g64.get_state()):
+            num += float(np.sum((ar - br) ** 2 + (ai - bi) ** 2))
+            den += float(np.sum(br ** 2 + bi ** 2))
+        e64, em = g64.energy(), gm.energy()
+        f64, fm = g64.friction()[2], gm.friction()[2]
+        rows.append({"steps": mark, "state_rel_l2": math.sqrt(num / den), "energy_rel": abs(em - e64) / e64,
+                     "friction_rel": abs(fm - f64) / f64})
     g64.close()
     gm.close()
+    out = {"pipe": d, **rows[-1], "at_steps": rows}
     return out
 
 
@@ -510,7 +518,7 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=16)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--plain-pipes", type=int, default=64)
-    ap.add_argument("--err-steps", type=int, default=100)
+    ap.add_argument("--err-steps", type=int, default=1000)
     ap.add_argument("--cfg2-spinup", type=int, default=50)
     ap.add_argument("--cfg2-steps", type=int, default=200)
     ap.add_argument("--no-cfg2", dest="with_cfg2", action="store_false")
