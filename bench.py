@@ -182,8 +182,11 @@ def read_traffic(kernel: str, workload: str):
 
 # algorithmic bytes of one launch of each kernel category, in units of the
 # coll field size S: the coll fields it must read and write once (factors,
-# twiddles and transform scratch are not algorithmic)
-PER_LAUNCH_S = {"lusolve": 2, "stencil": 2, "ew": 2, "infl": 4, "zinv": 3, "thinv": 3, "thfwd": 3,
+# twiddles and transform scratch are not algorithmic).  The fused step times
+# two banded-solve spans per half-step, the pressure solve (its right-hand
+# side in, the pressure out: 2S) and the three Helmholtz solves (3S in, 3S
+# out); "lusolve" is their mean, 4S.
+PER_LAUNCH_S = {"lusolve": 4, "stencil": 2, "ew": 2, "infl": 4, "zinv": 3, "thinv": 3, "thfwd": 3,
                 "zfwd": 3, "step": 10, "factor": 0}
 
 
