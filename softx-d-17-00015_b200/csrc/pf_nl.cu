@@ -275,16 +275,28 @@ __device__ __forceinline__ void nl_zfwd_body(const NLArgs &a, int bx, int by, in
     }
 }
 
+// Resident blocks per SM the transform kernels are compiled for.  In FP32
+// the register caps these imply cost a few spilled bytes and the extra warps
+// hide the passes' barrier and shared-memory latency (measured: 4.94 ms ->
+// 4.73 ms per 64-pipe mixed batch step).  FP64 rows need their registers:
+// 0 sets no minimum, leaving the compiler's own register choice.
+template <typename C> struct NLOcc {
+    static constexpr int zinv = 0, theta = 0, zfwd = 0;
+};
+template <> struct NLOcc<float2> {
+    static constexpr int zinv = 5, theta = 6, zfwd = 5;
+};
+
 template <int ZL, typename C>
-__global__ void __launch_bounds__(NL_THREADS) k_nl_zinv(NLArgs a) {
+__global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::zinv) k_nl_zinv(NLArgs a) {
     nl_zinv_body<ZL, C>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int TL, typename C>
-__global__ void __launch_bounds__(NL_THREADS) k_nl_theta(NLArgs a) {
+__global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::theta) k_nl_theta(NLArgs a) {
     nl_theta_body<TL, C>(a, blockIdx.x, blockIdx.y);
 }
 template <int ZL, typename C>
-__global__ void __launch_bounds__(NL_THREADS) k_nl_zfwd(NLArgs a) {
+__global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::zfwd) k_nl_zfwd(NLArgs a) {
     nl_zfwd_body<ZL, C>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -565,7 +577,7 @@ __global__ void __launch_bounds__(128) k_nl_mean64_fin(NLArgs a) {
 // stage for different lengths are independent and run concurrently (forked
 // onto auxiliary streams, joined before the next stage).
 template <int ZL, typename C>
-__global__ void __launch_bounds__(NL_THREADS) k_nl_zinv_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
+__global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::zinv) k_nl_zinv_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
     const int2 pb = blk[blockIdx.x];
     const NLArgs a = args[pb.x];  // by value: stores through its pointers cannot alias it
     const int gx = (a.g.M + a.MC - 1) / a.MC;
@@ -573,7 +585,7 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_zinv_b(const NLArgs *__restri
 }
 
 template <int TL, typename C>
-__global__ void __launch_bounds__(NL_THREADS) k_nl_theta_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
+__global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::theta) k_nl_theta_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
     const int2 pb = blk[blockIdx.x];
     const NLArgs a = args[pb.x];
     const int gx = (a.g.Z + a.ZC - 1) / a.ZC;
@@ -581,7 +593,7 @@ __global__ void __launch_bounds__(NL_THREADS) k_nl_theta_b(const NLArgs *__restr
 }
 
 template <int ZL, typename C>
-__global__ void __launch_bounds__(NL_THREADS) k_nl_zfwd_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
+__global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::zfwd) k_nl_zfwd_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
     const int2 pb = blk[blockIdx.x];
     const NLArgs a = args[pb.x];
     const int gx = (a.g.M + a.MC - 1) / a.MC;

@@ -181,8 +181,11 @@ __device__ __forceinline__ void step_rhs_body(const StepArgs &a, int hb) {
 // D columns ahead into a per-thread shared-memory ring with cp.async (8-byte
 // copies, one commit group per column), so each step of the sequential
 // sweep reads shared memory instead of waiting on DRAM.  The ring is laid out
-// [slot][value][thread] so consecutive threads hit consecutive banks.
-static constexpr int RING = 8;
+// [slot][value][thread] so consecutive threads hit consecutive banks.  Six
+// columns ahead, with the register budgets the launch bounds below set (four
+// Helmholtz blocks and eight pressure blocks per SM), measured fastest: deeper
+// rings or register queues cost more in resident warps than they hide.
+static constexpr int RING = 6;
 
 __device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -606,9 +609,9 @@ __device__ __forceinline__ void step_final_body(const StepArgs &a, int bx) {
 // per stage over the tiles of every pipe, blk[b] = (pipe, tile of that pipe).
 template <int RPT>
 __global__ void __launch_bounds__(HM *HR, 3) k_step_rhs(StepArgs a) { step_rhs_body<RPT>(a, blockIdx.x); }
-__global__ void __launch_bounds__(64) k_solve_pnp(StepArgs a) { solve_pnp_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(64, 8) k_solve_pnp(StepArgs a) { solve_pnp_body(a, blockIdx.x); }
 __global__ void k_step_proj(StepArgs a) { step_proj_body(a, blockIdx.x, blockIdx.y); }
-__global__ void __launch_bounds__(192) k_solve_ld(StepArgs a) { solve_ld_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(192, 4) k_solve_ld(StepArgs a) { solve_ld_body(a, blockIdx.x); }
 __global__ void __launch_bounds__(TM *TR) k_step_final(StepArgs a) { step_final_body(a, blockIdx.x); }
 
 #define PF_BATCH1(NAME, BODY, BOUNDS)                                                          \
@@ -617,8 +620,8 @@ __global__ void __launch_bounds__(TM *TR) k_step_final(StepArgs a) { step_final_
         const StepArgs a = args[pb.x]; /* by value: stores cannot alias it */                  \
         BODY(a, pb.y);                                                                         \
     }
-PF_BATCH1(k_solve_pnp_batch, solve_pnp_body, __launch_bounds__(64))
-PF_BATCH1(k_solve_ld_batch, solve_ld_body, __launch_bounds__(192))
+PF_BATCH1(k_solve_pnp_batch, solve_pnp_body, __launch_bounds__(64, 8))
+PF_BATCH1(k_solve_ld_batch, solve_ld_body, __launch_bounds__(192, 4))
 PF_BATCH1(k_step_final_batch, step_final_body, __launch_bounds__(TM *TR))
 #undef PF_BATCH1
 
