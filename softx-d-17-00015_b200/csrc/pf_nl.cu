@@ -278,10 +278,11 @@ __device__ __forceinline__ void nl_zfwd_body(const NLArgs &a, int bx, int by, in
 // Resident blocks per SM the transform kernels are compiled for.  In FP32
 // the register caps these imply cost a few spilled bytes and the extra warps
 // hide the passes' barrier and shared-memory latency (measured: 4.94 ms ->
-// 4.73 ms per 64-pipe mixed batch step).  FP64 rows need their registers:
-// 0 sets no minimum, leaving the compiler's own register choice.
+// 4.73 ms per 64-pipe mixed batch step).  In FP64 three blocks (80
+// registers) are the best trade (the single N=64 K=128 M=48 pipe: 1.258 ->
+// 1.21 ms per step); four spill too much.
 template <typename C> struct NLOcc {
-    static constexpr int zinv = 0, theta = 0, zfwd = 0;
+    static constexpr int zinv = 3, theta = 3, zfwd = 3;
 };
 template <> struct NLOcc<float2> {
     static constexpr int zinv = 5, theta = 6, zfwd = 5;
