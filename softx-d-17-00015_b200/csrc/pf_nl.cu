@@ -275,29 +275,31 @@ __device__ __forceinline__ void nl_zfwd_body(const NLArgs &a, int bx, int by, in
     }
 }
 
-// Resident blocks per SM the transform kernels are compiled for.  In FP32
-// the register caps these imply cost a few spilled bytes and the extra warps
+// Resident blocks per SM the transform kernels are compiled for.  In FP32,
+// up to length 192, the register caps these imply cost a few spilled bytes
+// and the extra warps
 // hide the passes' barrier and shared-memory latency (measured: 4.94 ms ->
-// 4.73 ms per 64-pipe mixed batch step).  In FP64 three blocks (80
-// registers) are the best trade (the single N=64 K=128 M=48 pipe: 1.258 ->
-// 1.21 ms per step); four spill too much.
-template <typename C> struct NLOcc {
-    static constexpr int zinv = 3, theta = 3, zfwd = 3;
+// 4.73 ms per 64-pipe mixed batch step).  In FP64, for transform lengths
+// of 144 and more, three blocks (80 registers) are the best trade (the
+// single N=64 K=128 M=48 pipe: 1.258 -> 1.21 ms per step); shorter FP64
+// rows keep the compiler's own register choice (0: no minimum).
+template <typename C, int L> struct NLOcc {
+    static constexpr int zinv = L >= 144 ? 3 : 0, theta = L >= 144 ? 3 : 0, zfwd = L >= 144 ? 3 : 0;
 };
-template <> struct NLOcc<float2> {
-    static constexpr int zinv = 5, theta = 6, zfwd = 5;
+template <int L> struct NLOcc<float2, L> {
+    static constexpr int zinv = L <= 192 ? 5 : 0, theta = L <= 192 ? 6 : 0, zfwd = L <= 192 ? 5 : 0;
 };
 
 template <int ZL, typename C>
-__global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::zinv) k_nl_zinv(NLArgs a) {
+__global__ void __launch_bounds__(NL_THREADS, (NLOcc<C, ZL>::zinv)) k_nl_zinv(NLArgs a) {
     nl_zinv_body<ZL, C>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int TL, typename C>
-__global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::theta) k_nl_theta(NLArgs a) {
+__global__ void __launch_bounds__(NL_THREADS, (NLOcc<C, TL>::theta)) k_nl_theta(NLArgs a) {
     nl_theta_body<TL, C>(a, blockIdx.x, blockIdx.y);
 }
 template <int ZL, typename C>
-__global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::zfwd) k_nl_zfwd(NLArgs a) {
+__global__ void __launch_bounds__(NL_THREADS, (NLOcc<C, ZL>::zfwd)) k_nl_zfwd(NLArgs a) {
     nl_zfwd_body<ZL, C>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -578,7 +580,7 @@ __global__ void __launch_bounds__(128) k_nl_mean64_fin(NLArgs a) {
 // stage for different lengths are independent and run concurrently (forked
 // onto auxiliary streams, joined before the next stage).
 template <int ZL, typename C>
-__global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::zinv) k_nl_zinv_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
+__global__ void __launch_bounds__(NL_THREADS, (NLOcc<C, ZL>::zinv)) k_nl_zinv_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
     const int2 pb = blk[blockIdx.x];
     const NLArgs a = args[pb.x];  // by value: stores through its pointers cannot alias it
     const int gx = (a.g.M + a.MC - 1) / a.MC;
@@ -586,7 +588,7 @@ __global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::zinv) k_nl_zinv_b(const 
 }
 
 template <int TL, typename C>
-__global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::theta) k_nl_theta_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
+__global__ void __launch_bounds__(NL_THREADS, (NLOcc<C, TL>::theta)) k_nl_theta_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
     const int2 pb = blk[blockIdx.x];
     const NLArgs a = args[pb.x];
     const int gx = (a.g.Z + a.ZC - 1) / a.ZC;
@@ -594,7 +596,7 @@ __global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::theta) k_nl_theta_b(cons
 }
 
 template <int ZL, typename C>
-__global__ void __launch_bounds__(NL_THREADS, NLOcc<C>::zfwd) k_nl_zfwd_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
+__global__ void __launch_bounds__(NL_THREADS, (NLOcc<C, ZL>::zfwd)) k_nl_zfwd_b(const NLArgs *__restrict__ args, const int2 *__restrict__ blk) {
     const int2 pb = blk[blockIdx.x];
     const NLArgs a = args[pb.x];
     const int gx = (a.g.M + a.MC - 1) / a.MC;
