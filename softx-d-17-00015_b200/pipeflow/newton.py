@@ -692,8 +692,16 @@ class Orbit(NewtonState):
         return res
 
     def close(self) -> None:
-        """Give the pipe back its own stream."""
+        """Give the pipe back its own stream (the orbit's stream is freed
+        with the Orbit, so the pipe must not keep using it)."""
         if self.ctx:
             self.stream.synchronize()
             _check(self.lib.pf_ctx_set_stream(self.ctx, None))
             self.ctx = None
+
+    def __del__(self):
+        try:
+            if self.ctx and self.pipe.ctx:
+                self.close()
+        except Exception:
+            pass
