@@ -239,6 +239,9 @@ int pf_steporbit(pf_ctx *ctx, int nsteps);
  * (mode-major, then radial point, then ur/ut/uz Re/Im).  The calls work
  * through the context's velocity fields (vel_ur, vel_ut, vel_uz), as the
  * reference's routines do, and leave them holding the last state handled. */
+/* The first call also fixes the alpha of the weights w: rtz2vec computes
+ * them once (newton.f90:580-587), so they stay when a continuation in alpha
+ * reconfigures the context. */
 int pf_orbit_set_scales(pf_ctx *ctx, const double *scaleU, double scaleT); /* newton.f90:272-305 */
 int pf_orbit_vec_len(const pf_ctx *ctx, long long *n);                     /* newton.f90:36 */
 int pf_orbit_rtz2vec(pf_ctx *ctx, double *v);                              /* newton.f90:567-602 */

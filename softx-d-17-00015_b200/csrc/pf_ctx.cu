@@ -207,7 +207,7 @@ static int ctx_init(pf_ctx *ctx, const pf_config *cfg, int device) {
     std::memset(&ctx->tim, 0, sizeof(ctx->tim));
     ctx->tim.t = 0.0;
     ctx->tim.dt = cfg->dt;
-    ctx->tim.pcn = -1;
+    ctx->tim.pcn = ctx->util_kind == PF_UTIL_CARREAU_YASUDA ? 1 : -1;  // the plug-in's one corrector pass
     ctx->lasterr = 1e99;
     ctx->newdt_i = 0;
     ctx->vel_nu = 1.0;
@@ -259,7 +259,7 @@ extern "C" int pf_ctx_reconfigure(pf_ctx *ctx, const pf_config *cfg) {
     // tim_precompute (timestep.f90:29-40)
     std::memset(&ctx->tim, 0, sizeof(ctx->tim));
     ctx->tim.dt = cfg->dt;
-    ctx->tim.pcn = -1;
+    ctx->tim.pcn = ctx->util_kind == PF_UTIL_CARREAU_YASUDA ? 1 : -1;  // the plug-in's one corrector pass
     ctx->lasterr = 1e99;
     ctx->newdt_i = 0;
     ctx->vel_nu = 1.0;

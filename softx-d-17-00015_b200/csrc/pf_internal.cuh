@@ -166,6 +166,7 @@ struct pf_ctx {
     double *mpart;       // FP64 mean-mode partial sums [ceil(H/32)][N][3]
     // Newton-Krylov vectors (newton.f90:36-37): scaleU, scaleT, dot partials
     double orbit_scaleU[3], orbit_scaleT;
+    double orbit_walpha;  // alpha of the vector weights, fixed when the scales are set
     bool orbit_set;
     double *orbit_red;   // ORBIT_DOT_BLOCKS + 1 doubles
     // util plug-in (var_null hook of main.f90): built-in kind, its

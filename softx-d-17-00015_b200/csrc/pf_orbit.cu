@@ -16,6 +16,7 @@
 
 struct OrbitScale {
     double s1, s2, s3;
+    double walpha;  // alpha in the weights w (rtz2vec keeps its first weights, newton.f90:580-587)
 };
 
 // the three multipliers of mode nh at radial point n
@@ -24,7 +25,7 @@ __device__ __forceinline__ void orbit_scale(int nh, int n, const double *__restr
     int k, m;
     mode_km(nh, g.K, k, m);
     const double d = sqrt(fabs(intrdr[n]));
-    const double w = 4.0 / (4.0 + (g.alpha * abs(k)) + (double)(g.Mp * abs(m)));
+    const double w = 4.0 / (4.0 + (u.walpha * abs(k)) + (double)(g.Mp * abs(m)));
     a = d * w * u.s1;
     b = d * w * u.s2;
     c = (k == 0 && m == 0) ? d : d * w * u.s3;
@@ -124,7 +125,7 @@ static int orbit_ready(const pf_ctx *ctx) {
 }
 
 static OrbitScale scales(const pf_ctx *ctx) {
-    return OrbitScale{ctx->orbit_scaleU[0], ctx->orbit_scaleU[1], ctx->orbit_scaleU[2]};
+    return OrbitScale{ctx->orbit_scaleU[0], ctx->orbit_scaleU[1], ctx->orbit_scaleU[2], ctx->orbit_walpha};
 }
 
 static int rtz2vec(pf_ctx *ctx, double *v) {
@@ -157,6 +158,7 @@ extern "C" int pf_orbit_set_scales(pf_ctx *ctx, const double *scaleU, double sca
                "pf_orbit_set_scales: scaleU must be finite and nonzero");
     for (int c = 0; c < 3; ++c) ctx->orbit_scaleU[c] = scaleU[c];
     ctx->orbit_scaleT = scaleT;
+    if (!ctx->orbit_set) ctx->orbit_walpha = ctx->g.alpha;
     ctx->orbit_set = true;
     return PF_OK;
 }

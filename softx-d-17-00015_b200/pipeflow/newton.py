@@ -20,11 +20,13 @@ Entry points, named after the reference's routines:
 plus getrhs / multJ / multA / steporbit / dotprod / dotprod_ms / getshiftdir /
 rtz2vec / vec2rtz on device vectors, and get_eigen (newton.f90:868-979, the
 Arnoldi iteration of arnoldi.f on multA) for the Floquet spectrum of the
-converged orbit.  Parameter continuation (Ctnu) and the output files are not
-included.
+converged orbit, and parameter continuation in Re or alpha
+(start_continuation / continuation_run, newton.f90:89-170).  The output files
+are not included.
 """
 from __future__ import annotations
 
+import copy
 import ctypes as C
 import math
 from dataclasses import dataclass, field
@@ -363,7 +365,7 @@ class Orbit(NewtonState):
     tensors of ms*n entries, n = 8 + 6*N*H.  The pipe's work is moved onto a
     stream of its own that the vector arithmetic shares."""
 
-    def __init__(self, pipe: Pipe, ndts, shifts, T_fixed: bool = False, epsJ: float = 1e-6):
+    def __init__(self, pipe: Pipe, ndts, shifts, T_fixed: bool = False, epsJ: float = 1e-6, continuation=None):
         if not torch.cuda.is_available():
             raise PipeflowError(L.PF_ERR_NODEVICE, "Orbit: no CUDA device")
         self.pipe = pipe
@@ -382,12 +384,31 @@ class Orbit(NewtonState):
             raise PipeflowError(L.PF_ERR_ARG, "Orbit: one (theta shift, z shift, period) per shooting point")
         self.T_fixed = T_fixed
         self.epsJ = epsJ
+        # parameter continuation (params_ct.in): param "Re" (ctp 1) or
+        # "alpha" (ctp 2), first step ctdp0, Newton-count window ctntmn..ctntmx
+        self.Ctnu = continuation is not None
+        if self.Ctnu:
+            c = dict(continuation)
+            if c.get("param") not in ("Re", "alpha"):
+                raise PipeflowError(L.PF_ERR_ARG, "Orbit: continuation param must be 'Re' or 'alpha'")
+            self.ctp = 1 if c["param"] == "Re" else 2
+            self.ctdp0 = float(c.get("ctdp0", 0.01))
+            self.ctntmn = int(c.get("ctntmn", 3))
+            self.ctntmx = int(c.get("ctntmx", 8))
+            self.ctpsc = 1.0
+            self.ctstp = None
+            self.ctx_ = None
+            self._d0 = None
+            self._m = 150
+            self.cti = 0
         self.scaleU = np.ones(3)
         self.scaleT = 1.0
         with torch.cuda.stream(self.stream):
             self.new_x = torch.zeros(self.ms * self.n, dtype=torch.float64, device=self.dev)
             hdr = torch.tensor(np.asarray(shifts, dtype=np.float64).reshape(self.ms, 3), device=self.dev)
             self.new_x.view(self.ms, self.n)[:, :3] = hdr
+            if self.Ctnu:  # x(4::n) = the parameter (newton.f90:318-326)
+                self.new_x.view(self.ms, self.n)[:, 3] = self._parameter()
             self.new_fx = torch.zeros_like(self.new_x)
         self.history = []
 
@@ -426,9 +447,29 @@ class Orbit(NewtonState):
         _check(self.lib.pf_orbit_shiftdir(self.ctx, int(i), C.c_void_p(_ptr(x)), C.c_void_p(_ptr(s))))
         return s
 
+    def _parameter(self) -> float:
+        return float(self.pipe.cfg.Re if self.ctp == 1 else self.pipe.cfg.alpha)
+
+    def _set_parameter(self, v: float) -> None:
+        """d_Re or d_alpha = v and var_precompute (newton.f90:730-735),
+        through pf_ctx_reconfigure; steporbit then recomputes the matrices."""
+        if v == self._parameter():
+            return
+        if not (math.isfinite(v) and v > 0.0):
+            raise PipeflowError(L.PF_ERR_ARG, f"continuation parameter {v} out of range")
+        cfg = copy.copy(self.pipe.cfg)
+        if self.ctp == 1:
+            cfg.Re = v
+        else:
+            cfg.alpha = v
+        self.pipe.reconfigure(cfg)
+
     def steporbit(self, ndts: int, x: torch.Tensor, y: torch.Tensor) -> None:
-        """newton.f90:721-831 (no continuation, no output): y[8:] = the
-        state ndts steps from x, shifted back for ndts != 1."""
+        """newton.f90:721-831 (no output): y[8:] = the state ndts steps
+        from x, shifted back for ndts != 1; with continuation the parameter
+        x[3]*ctpsc is set first."""
+        if self.Ctnu and ndts != 1:
+            self._set_parameter(float(x[3].item()) * self.ctpsc)
         s = self.lib.pf_orbit_step(self.ctx, int(ndts), C.c_void_p(_ptr(x)), C.c_void_p(_ptr(y)))
         if s not in (L.PF_OK, L.PF_ERR_CONVERGE):
             _check(s)
@@ -566,6 +607,12 @@ class Orbit(NewtonState):
                     vals[2] = float(xh[2])
             with torch.cuda.stream(self.stream):
                 y[p * n:p * n + 3] = torch.tensor(vals, dtype=torch.float64, device=self.dev)
+        if self.Ctnu:  # the parameter row (newton.f90:462)
+            if self.ctstp is None:
+                raise PipeflowError(L.PF_ERR_STATE, "multJ: call start_continuation first")
+            v = self.dotprod_ms(1, self.ctstp, x)
+            with torch.cuda.stream(self.stream):
+                y.view(ms, n)[:, 3] = v
         return y
 
     def multA(self, x: torch.Tensor, y0: torch.Tensor, epsA: float) -> torch.Tensor:
@@ -665,10 +712,12 @@ class Orbit(NewtonState):
 
     # -- the main program's search (newton.f90:102-128) -----------------------
     def solve(self, m: int = 150, nits: int = 100, rel_err: float = 3e-6, delta: float = -1.0,
-              mndl: float = 1e-7, mxdl: float = 1e7, gtol: float = 1e-3) -> NewtonResult:
+              mndl: float = 1e-7, mxdl: float = 1e7, gtol: float = 1e-3, d: float | None = None) -> NewtonResult:
         """newtonhook from new_x with the tolerances of newton_params.in
-        (rel_err, del, mndl, mxdl relative to |x|)."""
-        d = self.dotprod_ms(-1, self.new_x, self.new_x)
+        (rel_err, del, mndl, mxdl relative to |x|, |x|^2 = d, by default
+        that of new_x now)."""
+        if d is None:
+            d = self.dotprod_ms(-1, self.new_x, self.new_x)
         sd = math.sqrt(d)
         tol = rel_err * sd
 
@@ -690,6 +739,78 @@ class Orbit(NewtonState):
                              state=self, sub=sub)
         self.stream.synchronize()
         return res
+
+    # -- parameter continuation (newton.f90:89-101, 102-170) -----------------
+    def start_continuation(self, x_second: torch.Tensor) -> None:
+        """The main program's set-up of a continuation (newton.f90:102-117):
+        x_second is the second solution (what load_ms_states(1) reads from
+        state10.cdf.in), its x[3] the parameter it was found at; the first
+        guess becomes new_x + ctdp0 (x_second - new_x), and the parameter
+        entries are scaled by ctpsc = parameter / |x|."""
+        if not self.Ctnu:
+            raise PipeflowError(L.PF_ERR_STATE, "start_continuation: the Orbit has no continuation")
+        n = self.n
+        d = self.dotprod_ms(-1, self.new_x, self.new_x)
+        self._d0 = d
+        with torch.cuda.stream(self.stream):
+            self.ctx_ = self.new_x.clone()
+            self.new_x = x_second.to(self.dev, torch.float64).clone()
+            self.ctstp = self.new_x - self.ctx_
+            if float(self.ctstp.abs().max().item()) == 0.0:
+                self.ctstp.view(self.ms, n)[:, 3] += 1.0
+            self.ctx_ = self.new_x.clone()
+            self.new_x = self.new_x + self.ctstp * self.ctdp0
+        self.ctpsc = self._parameter() / math.sqrt(d)
+        with torch.cuda.stream(self.stream):
+            for v in (self.new_x, self.ctstp, self.ctx_):
+                v.view(self.ms, n)[:, 3] /= self.ctpsc
+
+    def continue_step(self, res: NewtonResult) -> dict:
+        """After a converged point (newton.f90:128-170): the record of
+        newton.dat_ct (point, Newton its, Re, alpha, phase speed sum(x2)/sum(x3))
+        and the next guess along the branch, with the step grown by 1.1,
+        halved above ctntmx Newton iterations or doubled below ctntmn (and
+        ndts and the times rescaled as there when T is fixed)."""
+        n, ms = self.n, self.ms
+        self.cti += 1
+        hdr = self.new_x.view(ms, n)[:, :3].cpu().numpy()
+        rec = dict(cti=self.cti, nits=res.nits, Re=self.pipe.cfg.Re, alpha=self.pipe.cfg.alpha,
+                   c=float(hdr[:, 1].sum() / hdr[:, 2].sum()), info=res.info)
+        d = 1.1
+        if res.nits > self.ctntmx:
+            d = 0.5
+        if res.nits < self.ctntmn:
+            d = 2.0
+        with torch.cuda.stream(self.stream):
+            self.ctstp = self.new_x - self.ctx_
+            self.ctx_ = self.new_x.clone()
+            self.new_x = self.new_x + self.ctstp * d
+        if self.T_fixed:
+            d = 1.0
+            if res.gits > (2 * self._m) // 3:
+                d = 2.0
+            if res.gits < 10:
+                d = 0.5
+            self.ndts = [int(nd * d + 0.5) for nd in self.ndts]
+            with torch.cuda.stream(self.stream):
+                for v in (self.new_x, self.ctx_):
+                    v.view(ms, n)[:, :3] *= d
+        return rec
+
+    def continuation_run(self, npoints: int, m: int = 150, **solve_kwargs) -> list:
+        """newtonhook at npoints successive points of the branch, stopping at
+        the first that does not converge; returns their records."""
+        if self.ctstp is None:
+            raise PipeflowError(L.PF_ERR_STATE, "continuation_run: call start_continuation first")
+        self._m = m
+        out = []
+        for _ in range(npoints):
+            res = self.solve(m=m, d=self._d0, **solve_kwargs)
+            rec = self.continue_step(res)
+            out.append(rec)
+            if res.info != 0:
+                break
+        return out
 
     def close(self) -> None:
         """Give the pipe back its own stream (the orbit's stream is freed

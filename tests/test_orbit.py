@@ -334,3 +334,50 @@ def test_device_floquet_spectrum_matches_dense_linear_map():
     assert sr[0] == pytest.approx(math.log(abs(lams[0])) / 0.5, rel=1e-12)
     assert res["eigvecs"] is not None
     orb.close()
+
+
+@pytest.mark.gpu
+def test_device_continuation_in_re():
+    """Parameter continuation (newton.f90:89-170, 730-735): the start sets
+    new_x = x1 + ctdp0 (x2 - x1) with the parameter entries over ctpsc,
+    steporbit runs at Re = x[3]*ctpsc (against an oracle pipe built at that
+    Re), and multJ's fourth row is dotprod(ctstp, x)."""
+    from pipeflow.newton import Orbit
+    ndts, shifts = [6], [(0.0, 0.3, 0.06)]
+    o, st = _oracle_with_state(CFG)
+    g = device_pipe(CFG)
+    g.vel_matrices()
+    state_to_dev(g, st)
+    g.vel_imposesym()
+    orb = Orbit(g, ndts, shifts, continuation=dict(param="Re", ctdp0=0.5, ctntmn=3, ctntmx=8))
+    orb.set_scales([1.0, 1.0, 1.0], 1.0)
+    orb.rtz2vec(orb.new_x)
+    x1 = _np(orb.new_x).copy()
+    assert x1[3] == CFG["Re"]
+    d = float(np.dot(x1[8:], x1[8:]))
+    x2 = x1.copy()
+    x2[3] = CFG["Re"] + 100.0
+    x2[8:] *= 1.01
+    orb.start_continuation(torch.tensor(x2, device=orb.dev))
+    ctpsc = CFG["Re"] / math.sqrt(d)
+    assert orb.ctpsc == pytest.approx(ctpsc, rel=1e-12)
+    want = x2 + 0.5 * (x2 - x1)
+    want[3] /= ctpsc
+    assert rel(_np(orb.new_x), want) < 1e-14
+    # the time-T map at the parameter the vector carries
+    Re2 = float(_np(orb.new_x)[3]) * ctpsc
+    y = torch.zeros_like(orb.new_x)
+    orb.steporbit(ndts[0], orb.new_x, y)
+    assert g.cfg.Re == pytest.approx(Re2, rel=1e-14)
+    o2 = oracle_pipe(dict(CFG, Re=Re2))
+    oo = OO.Orbit(o2, list(ndts))
+    oo.scaleU, oo.scaleT = np.ones(3), 1.0
+    yo = np.zeros(oo.n)
+    oo.steporbit(ndts[0], _np(orb.new_x), yo)
+    assert rel(_np(y)[8:], yo[8:]) < 1e-10
+    # the parameter row of the Jacobian
+    orb.new_fx = orb.getrhs(orb.new_x)
+    dx = torch.tensor(np.random.default_rng(4).standard_normal(orb.n) * 1e-3, device=orb.dev)
+    jx = _np(orb.multJ(dx))
+    assert jx[3] == pytest.approx(float(_np(orb.ctstp) @ _np(dx)), rel=1e-12)
+    orb.close()
