@@ -285,7 +285,8 @@ int pf_util_set(pf_ctx *ctx, int kind, const double *params, int nparams);
 int pf_util_set_callback(pf_ctx *ctx, pf_util_fn fn, void *user);
 int pf_util(pf_ctx *ctx, int flag);
 /* nu at the wall (mean mode), min and max over the grid from the last
- * Carreau-Yasuda evaluation (write_Re_nu, nonnewtonian.f90:302-318) */
+ * Carreau-Yasuda evaluation (write_Re_nu, nonnewtonian.f90:302-318);
+ * PF_ERR_STATE before the first evaluation */
 int pf_util_nu_stats(pf_ctx *ctx, double *nu_wall, double *nu_min, double *nu_max);
 
 /* ------------------------------------------------------------ state files */

@@ -180,6 +180,7 @@ struct pf_ctx {
     pf_util_fn util_cb;
     void *util_user;
     double *util_diag_d;
+    unsigned long long util_evals;  // plug-in evaluations since pf_util_set
     unsigned long long *cflmax;  // 3*N CFL maxima of the last fused transform
     bool cfl_fused;              // cflmax is current (else use vel_r/t/z)
     int *anypiv;         // per LU set: 1 if dgbtf2 swapped any row

@@ -267,7 +267,10 @@ static int nonnewtonian(pf_ctx *ctx) {
 int pf_util_run(pf_ctx *ctx, int flag) {
     if (flag == 2) {
         if (ctx->util_kind == PF_UTIL_CORIOLIS) PF_TRY(coriolis(ctx));
-        else if (ctx->util_kind == PF_UTIL_CARREAU_YASUDA) PF_TRY(nonnewtonian(ctx));
+        else if (ctx->util_kind == PF_UTIL_CARREAU_YASUDA) {
+            PF_TRY(nonnewtonian(ctx));
+            ++ctx->util_evals;
+        }
     }
     if (ctx->util_cb) ctx->util_cb(ctx, flag, ctx->util_user);
     return PF_OK;
@@ -292,7 +295,10 @@ extern "C" int pf_util_set(pf_ctx *ctx, int kind, const double *params, int npar
         PF_ARG(params[0] > 0.0 && params[1] > 0.0 && params[2] > 0.0 && params[6] != 0.0,
                "pf_util_set: rho, radius, mu_0 must be > 0 and a nonzero");
         PF_TRY(ensure_scratch(ctx, 16, 10));
-        if (!ctx->util_diag_d) PF_TRY(pf_alloc(ctx, (void **)&ctx->util_diag_d, 4 * sizeof(double)));
+        if (!ctx->util_diag_d) {
+            PF_TRY(pf_alloc(ctx, (void **)&ctx->util_diag_d, 4 * sizeof(double)));
+            PF_CUDA(cudaMemsetAsync(ctx->util_diag_d, 0, 4 * sizeof(double), ctx->stream));
+        }
         ctx->tim.pcn = 1;  // one corrector pass per step (nonnewtonian.f90:66-67)
         ctx->tim.it = 0;
         break;
@@ -302,6 +308,7 @@ extern "C" int pf_util_set(pf_ctx *ctx, int kind, const double *params, int npar
     }
     for (int i = 0; i < 8; ++i) ctx->util_par[i] = (params && i < nparams) ? params[i] : 0.0;
     ctx->util_kind = kind;
+    ctx->util_evals = 0;
     pf_graphs_reset(ctx);
     return PF_OK;
 }
@@ -321,8 +328,8 @@ extern "C" int pf_util(pf_ctx *ctx, int flag) {
 
 extern "C" int pf_util_nu_stats(pf_ctx *ctx, double *nu_wall, double *nu_min, double *nu_max) {
     PF_ARG(ctx, "pf_util_nu_stats: null ctx");
-    if (ctx->util_kind != PF_UTIL_CARREAU_YASUDA) {
-        pf_set_error("pf_util_nu_stats: the Carreau-Yasuda plug-in is not set");
+    if (ctx->util_kind != PF_UTIL_CARREAU_YASUDA || !ctx->util_evals) {
+        pf_set_error("pf_util_nu_stats: no Carreau-Yasuda evaluation yet");
         return PF_ERR_STATE;
     }
     double h[3];
