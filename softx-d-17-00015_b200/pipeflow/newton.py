@@ -356,6 +356,58 @@ def logeig(wr: np.ndarray, wi: np.ndarray, t: float):
 
 
 # ---------------------------------------------------------------------------
+# parameter continuation (the main program of newton.f90)
+# ---------------------------------------------------------------------------
+def continuation_start(new_x, x_second, n: int, ms: int, ctdp0: float, param: float, d: float):
+    """newton.f90:102-117: from the first solution new_x and the second
+    x_second (entry 3 of each block the parameter they were found at), the
+    branch direction ctstp = x_second - new_x (a unit step in the parameter
+    if they are equal), the last point ctx_ = x_second, the first guess
+    x_second + ctdp0 ctstp, and the parameter entries divided by
+    ctpsc = param / sqrt(d).  Returns (new_x, ctstp, ctx_, ctpsc)."""
+    ctx_ = new_x.clone()
+    nx = x_second.clone()
+    ctstp = nx - ctx_
+    if float(ctstp.abs().max()) == 0.0:
+        ctstp.view(ms, n)[:, 3] += 1.0
+    ctx_ = nx.clone()
+    nx = nx + ctstp * ctdp0
+    ctpsc = param / math.sqrt(d)
+    for v in (nx, ctstp, ctx_):
+        v.view(ms, n)[:, 3] /= ctpsc
+    return nx, ctstp, ctx_, ctpsc
+
+
+def continuation_next(new_x, ctx_, nits: int, gits: int, ctntmn: int, ctntmx: int, n: int, ms: int, ndts,
+                      T_fixed: bool, m: int):
+    """newton.f90:155-170: the next guess along the branch after a point
+    found in nits Newton iterations: the last step scaled by 1.1, by 0.5
+    above ctntmx iterations or by 2 below ctntmn; with a fixed period the
+    steps per period and the shifts and periods of new_x and ctx_ scaled by
+    2 (more than 2m/3 GMRES iterations) or 0.5 (fewer than 10).  Returns
+    (new_x, ctstp, ctx_, ndts)."""
+    d = 1.1
+    if nits > ctntmx:
+        d = 0.5
+    if nits < ctntmn:
+        d = 2.0
+    ctstp = new_x - ctx_
+    ctx_ = new_x.clone()
+    nx = new_x + ctstp * d
+    ndts = list(ndts)
+    if T_fixed:
+        d = 1.0
+        if gits > (2 * m) // 3:
+            d = 2.0
+        if gits < 10:
+            d = 0.5
+        ndts = [int(nd * d + 0.5) for nd in ndts]
+        for v in (nx, ctx_):
+            v.view(ms, n)[:, :3] *= d
+    return nx, ctstp, ctx_, ndts
+
+
+# ---------------------------------------------------------------------------
 # the orbit module (newton.f90)
 # ---------------------------------------------------------------------------
 class Orbit(NewtonState):
@@ -749,21 +801,11 @@ class Orbit(NewtonState):
         entries are scaled by ctpsc = parameter / |x|."""
         if not self.Ctnu:
             raise PipeflowError(L.PF_ERR_STATE, "start_continuation: the Orbit has no continuation")
-        n = self.n
         d = self.dotprod_ms(-1, self.new_x, self.new_x)
         self._d0 = d
         with torch.cuda.stream(self.stream):
-            self.ctx_ = self.new_x.clone()
-            self.new_x = x_second.to(self.dev, torch.float64).clone()
-            self.ctstp = self.new_x - self.ctx_
-            if float(self.ctstp.abs().max().item()) == 0.0:
-                self.ctstp.view(self.ms, n)[:, 3] += 1.0
-            self.ctx_ = self.new_x.clone()
-            self.new_x = self.new_x + self.ctstp * self.ctdp0
-        self.ctpsc = self._parameter() / math.sqrt(d)
-        with torch.cuda.stream(self.stream):
-            for v in (self.new_x, self.ctstp, self.ctx_):
-                v.view(self.ms, n)[:, 3] /= self.ctpsc
+            self.new_x, self.ctstp, self.ctx_, self.ctpsc = continuation_start(
+                self.new_x, x_second.to(self.dev, torch.float64), self.n, self.ms, self.ctdp0, self._parameter(), d)
 
     def continue_step(self, res: NewtonResult) -> dict:
         """After a converged point (newton.f90:128-170): the record of
@@ -776,25 +818,10 @@ class Orbit(NewtonState):
         hdr = self.new_x.view(ms, n)[:, :3].cpu().numpy()
         rec = dict(cti=self.cti, nits=res.nits, Re=self.pipe.cfg.Re, alpha=self.pipe.cfg.alpha,
                    c=float(hdr[:, 1].sum() / hdr[:, 2].sum()), info=res.info)
-        d = 1.1
-        if res.nits > self.ctntmx:
-            d = 0.5
-        if res.nits < self.ctntmn:
-            d = 2.0
         with torch.cuda.stream(self.stream):
-            self.ctstp = self.new_x - self.ctx_
-            self.ctx_ = self.new_x.clone()
-            self.new_x = self.new_x + self.ctstp * d
-        if self.T_fixed:
-            d = 1.0
-            if res.gits > (2 * self._m) // 3:
-                d = 2.0
-            if res.gits < 10:
-                d = 0.5
-            self.ndts = [int(nd * d + 0.5) for nd in self.ndts]
-            with torch.cuda.stream(self.stream):
-                for v in (self.new_x, self.ctx_):
-                    v.view(ms, n)[:, :3] *= d
+            self.new_x, self.ctstp, self.ctx_, self.ndts = continuation_next(
+                self.new_x, self.ctx_, res.nits, res.gits, self.ctntmn, self.ctntmx, n, ms, self.ndts, self.T_fixed,
+                self._m)
         return rec
 
     def continuation_run(self, npoints: int, m: int = 150, **solve_kwargs) -> list:

@@ -381,3 +381,44 @@ def test_device_continuation_in_re():
     jx = _np(orb.multJ(dx))
     assert jx[3] == pytest.approx(float(_np(orb.ctstp) @ _np(dx)), rel=1e-12)
     orb.close()
+
+
+def test_continuation_arithmetic():
+    """newton.f90:102-117 and 155-170 on host tensors: the start from two
+    solutions, the scaled parameter entries, the step-size rule and the
+    fixed-period rescaling."""
+    from pipeflow.newton import continuation_next, continuation_start
+    n, ms = 12, 2
+    rng = np.random.default_rng(7)
+    x1 = rng.standard_normal(n * ms)
+    x2 = x1 + 0.1 * rng.standard_normal(n * ms)
+    x1[3::n] = 2000.0
+    x2[3::n] = 2100.0
+    d = 4.0
+    nx, st, cx, ctpsc = continuation_start(torch.tensor(x1), torch.tensor(x2), n, ms, 0.25, 2000.0, d)
+    assert ctpsc == 2000.0 / 2.0
+    want_st = x2 - x1
+    want_nx = x2 + 0.25 * want_st
+    want_cx = x2.copy()
+    for w in (want_st, want_nx, want_cx):
+        w[3::n] /= ctpsc
+    assert np.allclose(st.numpy(), want_st, rtol=0, atol=1e-14)
+    assert np.allclose(nx.numpy(), want_nx, rtol=0, atol=1e-12)
+    assert np.array_equal(cx.numpy(), want_cx)
+    # equal solutions: a unit step in the parameter
+    _, st0, _, _ = continuation_start(torch.tensor(x1), torch.tensor(x1), n, ms, 0.25, 2000.0, d)
+    assert np.array_equal(st0.numpy()[3::n], np.full(ms, 1.0 / ctpsc))
+    # step rule: 1.1, 0.5 above ctntmx Newton iterations, 2 below ctntmn
+    for nits, f in ((5, 1.1), (9, 0.5), (2, 2.0)):
+        a, s, c, nd = continuation_next(torch.tensor(x2), torch.tensor(x1), nits, 50, 3, 8, n, ms, [100, 50],
+                                        False, 150)
+        assert np.allclose(a.numpy(), x2 + f * (x2 - x1), rtol=0, atol=1e-12)
+        assert np.array_equal(c.numpy(), x2) and nd == [100, 50]
+    # fixed period: GMRES iterations above 2m/3 double the steps per period and the times
+    a, s, c, nd = continuation_next(torch.tensor(x2), torch.tensor(x1), 5, 120, 3, 8, n, ms, [100, 51], True, 150)
+    assert nd == [200, 102]
+    want = x2 + 1.1 * (x2 - x1)
+    for p in range(ms):
+        want[p * n:p * n + 3] *= 2.0
+    assert np.allclose(a.numpy(), want, rtol=0, atol=1e-12)
+    assert np.allclose(c.numpy()[0:3], 2.0 * x2[0:3], rtol=0, atol=1e-15)
