@@ -25,11 +25,13 @@ def harmonics(K: int, M: int) -> int:
     return (2 * K - 1) * M - (K - 1)
 
 
-def write_like_reference(path, N, K, M, Mp, r, state, t=0.0, Re=0.0, alpha=0.0, dt=0.0, dtcor=0.0, dtcfl=0.0):
+def write_like_reference(path, N, K, M, Mp, r, state, t=0.0, Re=0.0, alpha=0.0, dt=0.0, dtcor=0.0, dtcfl=0.0,
+                         version=1):
     """A state file with io_save_state's definitions, in its order
-    (io.f90:315-348); Fortran dims (r, H, ReIm) are (ReIm, H, r) in C order."""
+    (io.f90:315-348); Fortran dims (r, H, ReIm) are (ReIm, H, r) in C order.
+    version 1: classic format, 2: 64-bit offsets."""
     H = harmonics(K, M)
-    f = scipy.io.netcdf_file(path, "w", version=1)
+    f = scipy.io.netcdf_file(path, "w", version=version)
     f.t = np.float64(t)
     f.Re = np.float64(Re)
     f.alpha = np.float64(alpha)

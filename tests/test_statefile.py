@@ -42,13 +42,14 @@ def test_written_file_is_netcdf_with_reference_structure(tmp_path):
         assert np.array_equal(data[0].T, re) and np.array_equal(data[1].T, im)
 
 
-def test_read_same_resolution_is_exact(tmp_path):
+@pytest.mark.parametrize("version", [1, 2], ids=["classic", "64bit_offset"])
+def test_read_same_resolution_is_exact(tmp_path, version):
     from pipeflow.statefile import state_read
     N, K, M, Mp = 16, 4, 5, 1
     r = _mesh(N)
     st = _state(N, K, M, 2)
     p = str(tmp_path / "state.cdf.in")
-    IO.write_like_reference(p, N, K, M, Mp, r, st, t=3.0, Re=2000.0, alpha=1.25, dt=0.005)
+    IO.write_like_reference(p, N, K, M, Mp, r, st, t=3.0, Re=2000.0, alpha=1.25, dt=0.005, version=version)
     got, sc, ch = state_read(p, N, K, M, Mp, r)
     assert ch == 0
     assert sc["t"] == 3.0 and sc["dt"] == 0.005 and sc["Re"] == 2000.0
