@@ -117,6 +117,13 @@ def test_missing_file_and_wrong_mp_are_errors(tmp_path):
     IO.write_like_reference(p, 8, 2, 4, 2, _mesh(8), _state(8, 2, 4, 5))
     with pytest.raises(P.PipeflowError, match="Mp"):
         state_read(p, 8, 2, 4, 1, _mesh(8))
+    # a truncated file and a file that is not netCDF are errors, not crashes
+    data = open(p, "rb").read()
+    for k, blob in enumerate((data[:len(data) // 2], data[:40], b"not a netCDF file at all")):
+        q = str(tmp_path / f"bad{k}.cdf")
+        open(q, "wb").write(blob)
+        with pytest.raises(P.PipeflowError):
+            state_read(q, 8, 2, 4, 2, _mesh(8))
 
 
 @pytest.mark.gpu
