@@ -109,3 +109,32 @@ def test_callback_order_and_effect():
     assert no == ng
     assert O.rel_l2(state_from_dev(g), o.state()) <= 1e-11
     g.util_set_callback(None)
+
+
+def test_carreau_yasuda_on_laminar_flow_matches_the_stress_divergence():
+    """For Hagen-Poiseuille flow alone (u' = 0) the strain rate is |U'| = 2r
+    and the extra term is the divergence of the extra viscous stress,
+    N'_z(r) = [-4 (nu - 1) - 2 r nu'(r)] / Re in the mean mode, with nothing
+    in the other components or modes.  The radial derivatives are the 9-point
+    finite differences, so the first points off the axis carry a truncation
+    error that falls fast with N (1e-4 of the maximum at N = 40, 6e-7 at 80)."""
+    o = oracle_pipe(dict(N=80, K=3, M=3, Mp=1, Re=2000.0, alpha=1.25, dt=0.01))
+    o.vel_matrices()
+    z = O.Coll.zeros(o.N, o.H)
+    o.vel_Nr, o.vel_Nt, o.vel_Nz = z.copy(), z.copy(), z.copy()
+    o.vel_ur, o.vel_ut, o.vel_uz = z.copy(), z.copy(), z.copy()
+    # a relaxation time that keeps nu(r) smooth on the mesh (lam * 2r <= 10)
+    rho, radius, mu0, muinf, lamCY, nCY, aCY = 1000.0, 0.01, 0.05, 0.0035, 0.005, 0.36, 2.0
+    UO.carreau_yasuda(o, rho, radius, mu0, muinf, lamCY, nCY, aCY)
+    r = o.mes_D.r
+    lam = o.cfg.Re * lamCY * mu0 / (rho * radius ** 2)
+    e1, e2 = muinf / mu0, -nCY / aCY
+    x = lam * 2.0 * r
+    nu = e1 + (1 - e1) * (1 + x ** aCY) ** e2
+    dnu = (1 - e1) * e2 * (1 + x ** aCY) ** (e2 - 1) * aCY * x ** (aCY - 1) * lam * 2.0
+    want = (-4.0 * (nu - 1.0) - 2.0 * r * dnu) / o.cfg.Re
+    got = o.vel_Nz.re[:, 0]
+    assert np.max(np.abs(got - want)) < 2e-6 * np.max(np.abs(want))
+    assert np.max(np.abs(got - want)[r > 0.2]) < 1e-8 * np.max(np.abs(want))
+    assert np.max(np.abs(o.vel_Nr.re)) + np.max(np.abs(o.vel_Nt.re)) < 1e-9 * np.max(np.abs(want))
+    assert np.max(np.abs(o.vel_Nz.re[:, 1:])) + np.max(np.abs(o.vel_Nz.im)) < 1e-9 * np.max(np.abs(want))
