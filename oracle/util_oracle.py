@@ -6,7 +6,8 @@ a numpy restatement on top of the timestep oracle (pipeflow_oracle.Pipe).
 
 Parity status: **parity unpinned** (as the timestep oracle); the plug-ins are
 additionally pinned by invariants in tests/test_util.py (a Coriolis force
-about the pipe axis acts on the azimuthal and radial velocity only; a
+about the pipe axis acts on the azimuthal and radial velocity only, and on
+laminar flow it is the analytic m = 1 force; a
 Newtonian limit of the Carreau-Yasuda law, mu_inf = mu_0, adds nothing; on
 laminar flow the Carreau-Yasuda term equals the analytic divergence of the
 extra viscous stress).

@@ -138,3 +138,31 @@ def test_carreau_yasuda_on_laminar_flow_matches_the_stress_divergence():
     assert np.max(np.abs(got - want)[r > 0.2]) < 1e-8 * np.max(np.abs(want))
     assert np.max(np.abs(o.vel_Nr.re)) + np.max(np.abs(o.vel_Nt.re)) < 1e-9 * np.max(np.abs(want))
     assert np.max(np.abs(o.vel_Nz.re[:, 1:])) + np.max(np.abs(o.vel_Nz.im)) < 1e-9 * np.max(np.abs(want))
+
+
+def test_coriolis_on_laminar_flow_is_the_analytic_force():
+    """For Hagen-Poiseuille flow alone the Coriolis force -1/(4 Ro) Omega x U z
+    has only the m = 1, k = 0 mode: N_r = (1/2) d sin(phi) U i, N_t =
+    -(1/2) d sin(phi) U, with d = -1/(4 Ro), Ro = Re Ek0 (e^{+i theta}
+    coefficients of -d sin(phi) U sin(theta) and -d sin(phi) U cos(theta))."""
+    import math
+    o = oracle_pipe(dict(N=20, K=3, M=3, Mp=1, Re=2000.0, alpha=1.25, dt=0.01))
+    o.vel_matrices()
+    z = O.Coll.zeros(o.N, o.H)
+    o.vel_ur, o.vel_ut, o.vel_uz = z.copy(), z.copy(), z.copy()
+    o.vel_transform()
+    o.vel_nonlinear()
+    N0 = [o.vel_Nr.copy(), o.vel_Nt.copy(), o.vel_Nz.copy()]
+    Ek0, phi = 0.5, 0.3
+    UO.coriolis(o, Ek0, phi)
+    d = -1.0 / (4.0 * o.cfg.Re * Ek0)
+    a = 0.5 * d * math.sin(phi) * o.vel_U
+    nh = O.mode_index(o.K, 0, 1)
+    want_r = O.Coll.zeros(o.N, o.H)
+    want_r.im[:, nh] = a
+    want_t = O.Coll.zeros(o.N, o.H)
+    want_t.re[:, nh] = -a
+    tol = 1e-12 * float(np.max(np.abs(a)))
+    for got, base, want in ((o.vel_Nr, N0[0], want_r), (o.vel_Nt, N0[1], want_t), (o.vel_Nz, N0[2], z)):
+        assert np.max(np.abs(got.re - base.re - want.re)) < tol
+        assert np.max(np.abs(got.im - base.im - want.im)) < tol
