@@ -5,18 +5,25 @@
 // stream is being captured elsewhere, or a Fortran driver that only hands
 // over device pointers it allocated itself).
 //
-// Its scratch (the twiddle tables and the (m, z) intermediate of the z pass)
-// is the file-scope array below, PF_NOALLOC_SCRATCH_BYTES (24 MiB) in size;
-// every GPU that loads this library holds it until the process exits.  All
-// calls share it and it keeps the previous call's contents (nothing in it has
-// to start at zero: every call writes the twiddles and every scratch entry it
-// later reads).  Calls that overlap on the GPU -- on different streams, or
-// from different host threads without ordering -- race on it.
+// Its scratch is the file-scope array below, PF_NOALLOC_SCRATCH_BYTES
+// (24 MiB) in size; every GPU that loads this library holds it until the
+// process exits.  The first 64 KiB hold the twiddle tables of every built
+// transform length, written once per device at set-up; the rest holds the
+// (m, z) intermediate of the z pass.  All calls share the intermediate and it
+// keeps the previous call's contents (nothing in it has to start at zero:
+// every call writes every entry it later reads).  Calls that overlap on the
+// GPU -- on different streams, or from different host threads without
+// ordering -- race on it.
 //
 // Host code must not hand the array's name to a kernel: in host code the name
-// denotes a host-side stand-in.  The device address is looked up once per
-// device with cudaGetSymbolAddress (with that device current) on the first
-// call made on that device; make that first call before any stream capture.
+// denotes a host-side stand-in.  The first call made on a device, with that
+// device current, does the set-up: it looks up the device address with
+// cudaGetSymbolAddress and writes the twiddle tables with a synchronous copy.
+// Make that first call before any stream capture.  Every later call only
+// queues its two kernels on the caller's stream.  The address and the tables
+// are kept per device ordinal for the life of the process; a cudaDeviceReset
+// in the caller discards the tables, and this entry point is not usable on
+// that device after one.
 #include <cmath>
 #include <mutex>
 #include "pf_internal.cuh"
@@ -24,10 +31,32 @@
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[PF_NOALLOC_SCRATCH_BYTES];
 
-static constexpr size_t kTwiddleBytes = 64 * 1024;  // room for Z + Th <= 4096 complex
+static constexpr size_t kTwiddleBytes = 64 * 1024;  // tables of all built lengths (21 KiB used)
 static std::mutex g_noalloc_mu;
 static void *g_noalloc_addr[256];
 
+#define PF_NA_LENGTHS(X) X(12) X(15) X(18) X(24) X(36) X(48) X(72) X(96) X(144) X(192) X(288) X(384)
+static const int kLengths[] = {
+#define PF_CASE(L) L,
+    PF_NA_LENGTHS(PF_CASE)
+#undef PF_CASE
+};
+static constexpr int kNumLengths = (int)(sizeof(kLengths) / sizeof(kLengths[0]));
+
+// offset (in double2 entries) of length L's table exp(+2 pi i t/L), t < L,
+// in the twiddle region; -1 if L is not built
+static int twiddle_offset(int L) {
+    int off = 0;
+    for (int i = 0; i < kNumLengths; ++i) {
+        if (kLengths[i] == L) return off;
+        off += kLengths[i];
+    }
+    return -1;
+}
+
+// Set-up, once per device: the scratch address, and the twiddle tables of
+// every built length (rounded once from long double) written into its first
+// kTwiddleBytes with a synchronous copy from host memory.
 static int scratch_address(int dev, unsigned char **out) {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (dev < 0 || dev >= 256) {
@@ -39,6 +68,20 @@ static int scratch_address(int dev, unsigned char **out) {
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
             pf_set_error("pf_tra_coll2phys_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            return PF_ERR_CUDA;
+        }
+        std::vector<double2> tw;
+        for (int i = 0; i < kNumLengths; ++i) {
+            const int L = kLengths[i];
+            for (int t = 0; t < L; ++t) {
+                const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)t / (long double)L;
+                tw.push_back(make_double2((double)cosl(a), (double)sinl(a)));
+            }
+        }
+        static_assert(kTwiddleBytes >= 1329 * sizeof(double2), "twiddle region too small");
+        e = cudaMemcpy(p, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            pf_set_error("pf_tra_coll2phys_noalloc: twiddle set-up copy failed: %s", cudaGetErrorString(e));
             return PF_ERR_CUDA;
         }
         g_noalloc_addr[dev] = p;
@@ -124,8 +167,6 @@ __global__ void __launch_bounds__(256) k_na_thinv(const double2 *__restrict__ T,
     }
 }
 
-#define PF_NA_LENGTHS(X) X(12) X(15) X(18) X(24) X(36) X(48) X(72) X(96) X(144) X(192) X(288) X(384)
-
 static bool na_length_ok(int L) {
     switch (L) {
 #define PF_CASE(L) case L:
@@ -158,17 +199,10 @@ extern "C" int pf_tra_coll2phys_noalloc(int N, int K, int M, const double *re, c
     unsigned char *scratch = nullptr;
     PF_TRY(scratch_address(dev, &scratch));
     cudaStream_t st = (cudaStream_t)cuda_stream;
-    double2 *twz = reinterpret_cast<double2 *>(scratch);
-    double2 *twt = twz + Z;
+    const double2 *tables = reinterpret_cast<const double2 *>(scratch);
+    const double2 *twz = tables + twiddle_offset(Z);
+    const double2 *twt = tables + twiddle_offset(Th);
     double2 *T = reinterpret_cast<double2 *>(scratch + kTwiddleBytes);
-    // twiddles exp(+2 pi i t/L), rounded once from long double
-    std::vector<double2> tw(Z + Th);
-    for (int i = 0; i < Z + Th; ++i) {
-        const int L = i < Z ? Z : Th, t = i < Z ? i : i - Z;
-        const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)t / (long double)L;
-        tw[i] = make_double2((double)cosl(a), (double)sinl(a));
-    }
-    PF_CUDA(cudaMemcpyAsync(twz, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
     int MC = M;
     while (MC > 1 && (size_t)(2 * MC + 1) * Z * sizeof(double2) > 60 * 1024) --MC;
     const size_t zsm = (size_t)(2 * MC + 1) * Z * sizeof(double2);

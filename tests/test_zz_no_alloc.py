@@ -15,7 +15,10 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-CASES = [dict(N=40, K=24, M=16), dict(N=64, K=128, M=48), dict(N=16, K=5, M=4)]
+# together these run every built transform length (3K and 3M in 12, 15, 18,
+# 24, 36, 48, 72, 96, 144, 192, 288, 384) through the allocation-free kernels
+CASES = [dict(N=40, K=24, M=16), dict(N=64, K=128, M=48), dict(N=16, K=5, M=4),
+         dict(N=12, K=6, M=8), dict(N=20, K=12, M=32), dict(N=16, K=32, M=64), dict(N=10, K=4, M=96)]
 
 
 def _rel(a, b):
