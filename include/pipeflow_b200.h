@@ -43,6 +43,7 @@ extern "C" {
 #define PF_ERR_STATE    -5   /* call out of order (e.g. step before matrices) */
 #define PF_ERR_CONVERGE -6   /* corrector diverged / too many iterations    */
 #define PF_ERR_NODEVICE -7   /* no CUDA device visible                      */
+#define PF_ERR_CANCELLED -8  /* a served request was cancelled              */
 
 #define PF_KL 4              /* i_KL, parameters.f90:43 */
 
@@ -93,6 +94,24 @@ int pf_ctx_destroy(pf_ctx *ctx);
 int pf_ctx_reconfigure(pf_ctx *ctx, const pf_config *cfg);
 /* Run the context's work on an external cudaStream_t (NULL = own stream). */
 int pf_ctx_set_stream(pf_ctx *ctx, void *cuda_stream);
+
+/* Launch choices of a context's fused timestep.  No counterpart in the
+ * reference, whose only tuning is FFTW_PATIENT planning
+ * (transform.fftw3.f90:36-57).  Every choice gives the same numbers bit for
+ * bit; only the speed differs.  The autotuner (pipeflow.tune) sets them by
+ * timing the candidates per pipe shape.  A zero struct is the built-in
+ * choice.  Setting them drops the context's captured step graphs. */
+#define PF_LD_AUTO     0  /* the built-in choice (streamed factors) */
+#define PF_LD_STREAMED 1  /* Helmholtz factors streamed from HBM */
+#define PF_LD_REBUILT  2  /* Helmholtz factors rebuilt on chip (factorisations
+                             that did not pivot, N >= 10; else streamed) */
+typedef struct {
+    int ld_solver; /* PF_LD_* */
+    int nl_mc;     /* z-pass columns per block (1..M; 0 = built-in) */
+    int nl_zc;     /* theta-pass z rows per block (even, 2..32; 0 = built-in) */
+} pf_tuning;
+int pf_ctx_set_tuning(pf_ctx *ctx, const pf_tuning *t);
+int pf_ctx_get_tuning(const pf_ctx *ctx, pf_tuning *t);
 int pf_ctx_sync(pf_ctx *ctx);
 /* H = number of harmonics (i_H1+1), Z = 3K, Th = 3M. */
 int pf_ctx_dims(const pf_ctx *ctx, int *N, int *H, int *Z, int *Th);
@@ -153,8 +172,13 @@ int pf_tra_phys2coll(const pf_phys *p, pf_coll *c);
  * PF_NOALLOC_SCRATCH_BYTES per GPU: sizes with N*M*3K*16 + 64 KiB above it,
  * or with 3K or 3M outside {12,15,18,24,36,48,72,96,144,192,288,384}, are
  * rejected with PF_ERR_ARG.  All calls share the scratch, so calls that
- * overlap on the GPU race.  The first call on a device looks up the scratch
- * address (cudaGetSymbolAddress); make it before any stream capture. */
+ * overlap on the GPU race.  The first call on a device (with that device
+ * current) is its set-up: it looks up the scratch address
+ * (cudaGetSymbolAddress) and writes the twiddle tables of every built length
+ * into the scratch with one synchronous copy; make it before any stream
+ * capture.  Later calls only queue two kernels on cuda_stream.  The set-up is
+ * kept for the process's life: a cudaDeviceReset on that device makes the
+ * entry point unusable there. */
 #define PF_NOALLOC_SCRATCH_BYTES (24u * 1024u * 1024u)
 int pf_tra_coll2phys_noalloc(int N, int K, int M, const double *re, const double *im,
                              double *phys, void *cuda_stream);
@@ -266,13 +290,22 @@ int pf_diag_friction(pf_ctx *ctx, double *Ub, double *Uc, double *Ufr);
 /* ------------------------------------------------------------ util hook */
 /* The plug-in hook of main.f90: var_null(2) after every evaluation of the
  * nonlinear terms, var_null(1) once per step before the predictor
- * (main.f90:23,30,38); pf_timestep calls it when a plug-in is set (and then
- * runs eagerly, without its graphs; orbit steps, like newton.f90's
- * steporbit, do not call it).  Built-in plug-ins, on the device:
+ * (main.f90:23,30,38); pf_timestep calls it when a plug-in is set (orbit
+ * steps, like newton.f90's steporbit, do not call it).  The Coriolis and
+ * Carreau-Yasuda plug-ins are device work only and run inside the step's
+ * CUDA graphs; LES (its update_nu_r reads max nu_t back to the host) and a
+ * host callback make pf_timestep run eagerly.  Built-in plug-ins, on the
+ * device:
  *   PF_UTIL_CORIOLIS: params Ek0, phi -- Coriolis.f90:13-73 (Mp must be 1)
  *   PF_UTIL_CARREAU_YASUDA: params rho, radius, mu_0, mu_inf, lam_CY, n_CY,
  *     a_CY[, fc1] -- nonnewtonian.f90:32-246; sets one corrector pass per
  *     step (tim_pcn = 1) as the reference does
+ *   PF_UTIL_LES: params model (1 Smagorinsky, 2 Vreman), C_s, filter (1, 2,
+ *     3), A_plus -- the eddy-viscosity terms of LES.f90:102-339 (get_nu,
+ *     update_nu_r with its re-factorisation when the reference viscosity
+ *     moves, update_nonlin_terms); one corrector pass per step as there.
+ *     Its var_null(1) side (LES.f90:51-56: bisect, profiles, vel_Retau.dat)
+ *     is output and is not built.
  * A host callback fn(ctx, flag, user) runs after the built-in at both
  * flags, for plug-ins written against this ABI (adding to vel_Nr/Nt/Nz
  * through pf_vel_coll and pf_var_coll_add).  pf_util runs the hook once, for
@@ -280,12 +313,14 @@ int pf_diag_friction(pf_ctx *ctx, double *Ub, double *Uc, double *Ufr);
 #define PF_UTIL_NONE            0
 #define PF_UTIL_CORIOLIS        1
 #define PF_UTIL_CARREAU_YASUDA  2
+#define PF_UTIL_LES             3
 typedef void (*pf_util_fn)(pf_ctx *ctx, int flag, void *user);
 int pf_util_set(pf_ctx *ctx, int kind, const double *params, int nparams);
 int pf_util_set_callback(pf_ctx *ctx, pf_util_fn fn, void *user);
 int pf_util(pf_ctx *ctx, int flag);
 /* nu at the wall (mean mode), min and max over the grid from the last
- * Carreau-Yasuda evaluation (write_Re_nu, nonnewtonian.f90:302-318);
+ * Carreau-Yasuda or LES evaluation (write_Re_nu, nonnewtonian.f90:302-318;
+ * for LES, the eddy viscosity nu_t whose maximum is LES.f90's nu_max);
  * PF_ERR_STATE before the first evaluation */
 int pf_util_nu_stats(pf_ctx *ctx, double *nu_wall, double *nu_min, double *nu_max);
 
@@ -373,6 +408,10 @@ int pf_batch_io_sync(pf_batch *b);
  * time, so per-launch durations here include the sharing of the GPU. */
 int pf_batch_prof_enable(pf_batch *b, int mask);
 int pf_batch_prof_read(pf_batch *b, int cat, double *ms, unsigned long long *launches);
+/* Only the spans of the stage-batched launches (each covers every pipe of the
+ * batch), without the per-pipe launches such as one pipe's extra corrector
+ * pass: these are the spans whose bytes are the whole batch's. */
+int pf_batch_prof_read_staged(pf_batch *b, int cat, double *ms, unsigned long long *launches);
 /* Number of pipes, and membership changes.  A batch made with npipes = 0
  * starts empty.  pf_batch_attach adds a context the caller created and still
  * owns (same device; it must outlive its membership); pf_batch_detach removes
@@ -413,7 +452,18 @@ int pf_serve_submit(pf_server *s, const pf_config *cfg, int nsteps,
 int pf_serve_step(pf_server *s, int *admitted, int *finished);
 /* Ids finished since the last call (up to cap). */
 int pf_serve_finished(pf_server *s, long long *ids, int cap, int *n);
-/* Final state of a finished request; the request is forgotten afterwards. */
+/* Cancel a queued or running request: it leaves the queue or the batch at
+ * once (its context goes back to the pool) and is reported finished; its
+ * pf_serve_result returns PF_ERR_CANCELLED.  PF_ERR_STATE if the request has
+ * already finished, PF_ERR_ARG for an unknown id.  No reference routine: the
+ * reference runs one state per process. */
+int pf_serve_cancel(pf_server *s, long long id);
+/* Final state of a finished request; the request is forgotten afterwards.
+ * A request that failed returns its own error instead, alone: the corrector
+ * check's abort (PF_ERR_CONVERGE with tim_check_cgce's message,
+ * timestep.f90:222-240), a non-finite corrector error (a NaN or Inf in its
+ * state; PF_ERR_CONVERGE), a failed admission, or PF_ERR_CANCELLED.  The
+ * other requests of the batch are not affected. */
 int pf_serve_result(pf_server *s, long long id, double *ur_re, double *ur_im, double *ut_re,
                     double *ut_im, double *uz_re, double *uz_im);
 int pf_serve_stats(pf_server *s, int *queued, int *active, int *pooled, unsigned long long *bytes,
@@ -428,13 +478,15 @@ int pf_serve_batch(pf_server *s, pf_batch **b);
 #define PF_K_THINV    1   /* theta pass (c2r) -> physical                   */
 #define PF_K_THFWD    2   /* theta pass (r2c), fused u x curl(u)            */
 #define PF_K_ZFWD     3   /* z pass -> spectral, truncation                 */
-#define PF_K_LUSOLVE  4   /* banded solves                                   */
+#define PF_K_LUSOLVE  4   /* banded solves (the Helmholtz u+, u-, uz ones in
+                             the fused step)                                 */
 #define PF_K_STENCIL  5   /* meshmult / curl / grad / div / tim_meshmult    */
 #define PF_K_EW       6   /* elementwise, symmetry, reductions, transfers   */
 #define PF_K_INFL     7   /* influence correction, flux, addHPF             */
 #define PF_K_FACTOR   8   /* banded LU factorisation (vel_matrices)          */
 #define PF_K_STEP     9   /* fused per-mode step kernels                     */
-#define PF_K_NCAT    10
+#define PF_K_PPE     10   /* pressure-Poisson banded solve of the fused step */
+#define PF_K_NCAT    11
 /* Count of this library's kernel launches on the context since creation. */
 int pf_ctx_launches(const pf_ctx *ctx, unsigned long long *n);
 /* Event timing for the categories whose bit (1 << PF_K_*) is set in mask;

@@ -450,9 +450,22 @@ static long long batch_after_step(pf_batch *b, int orbit, int *status) {
     long long passes = 0;
     for (int i = 0; i < b->n; ++i) {
         pf_ctx *c = b->pipes[i];
-        c->tim.dterr = std::max(c->tim.dterr, std::sqrt(bits_to_double(b->hsc[i].dterr2_bits)));
+        const double err2 = bits_to_double(b->hsc[i].dterr2_bits);
+        c->tim.dterr = std::max(c->tim.dterr, std::sqrt(err2));
         c->tim.it = 1;
+        c->last_status = PF_OK;
+        c->last_error.clear();
         int s = pf_tim_check_cgce(c);
+        if (s != PF_OK) {
+            c->last_status = s;
+            c->last_error = pf_last_error();
+        }
+        // the state went non-finite: the max of the corrections' bit patterns
+        // is a NaN or Inf pattern (the reference would carry on with NaN)
+        if (!std::isfinite(err2) && c->last_status == PF_OK) {
+            c->last_status = PF_ERR_CONVERGE;
+            c->last_error = "non-finite corrector error: NaN or Inf in the state";
+        }
         ++passes;
         if (!orbit) {
             while (c->tim.it != 0) {  // further corrector passes for this pipe only
@@ -465,6 +478,10 @@ static long long batch_after_step(pf_batch *b, int orbit, int *status) {
                     break;
                 }
                 s = pf_tim_check_cgce(c);
+                if (s != PF_OK && c->last_status == PF_OK) {
+                    c->last_status = s;
+                    c->last_error = pf_last_error();
+                }
                 ++passes;
             }
             if (s != PF_OK) *status = s;
@@ -513,6 +530,8 @@ extern "C" int pf_batch_step(pf_batch *b, int nsteps, int orbit, long long *corr
                 } else {
                     int nc = 0;
                     const int s = pf_timestep(c, &nc);
+                    c->last_status = s;
+                    c->last_error = s != PF_OK ? pf_last_error() : "";
                     if (s != PF_OK) status = s;
                     passes += nc;
                 }
@@ -645,6 +664,15 @@ extern "C" int pf_batch_prof_read(pf_batch *b, int cat, double *ms, unsigned lon
     }
     if (ms) *ms = t + b->sprof.ms[cat];
     if (launches) *launches = n + b->sprof.n[cat];
+    return PF_OK;
+}
+
+// Device milliseconds and spans of category `cat` of the stage-batched
+// launches alone (every span covers all pipes of the batch).
+extern "C" int pf_batch_prof_read_staged(pf_batch *b, int cat, double *ms, unsigned long long *launches) {
+    PF_ARG(b && cat >= 0 && cat < PF_K_NCAT, "pf_batch_prof_read_staged: bad argument");
+    if (ms) *ms = b->sprof.ms[cat];
+    if (launches) *launches = b->sprof.n[cat];
     return PF_OK;
 }
 

@@ -192,7 +192,10 @@ static int ctx_init(pf_ctx *ctx, const pf_config *cfg, int device) {
     PF_TRY(pf_alloc(ctx, (void **)&ctx->cflmax, (size_t)3 * N * sizeof(unsigned long long)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->mpart, (size_t)((g.H + 31) / 32) * N * 3 * sizeof(double)));
     PF_TRY(pf_alloc(ctx, (void **)&ctx->anypiv, sizeof(int)));
-    ctx->T_bytes = (size_t)6 * N * g.M * g.Z * sizeof(double2);
+    // the (m, z) intermediate in FP64; in mixed precision its FP32 copy takes
+    // the first 6*N*M*Z float2 and the FP32 curl(u) fields (3*N*Hp float2) follow
+    ctx->T_bytes = std::max((size_t)6 * N * g.M * g.Z * sizeof(double2),
+                            ((size_t)6 * N * g.M * g.Z + (size_t)3 * N * g.Hp) * sizeof(float2));
     PF_TRY(pf_alloc(ctx, &ctx->T, ctx->T_bytes));
     // LU factor storage for the four matrix sets
     pf_lumesh *L[4] = {&ctx->LNp, &ctx->LDp, &ctx->LDm, &ctx->LDz};
@@ -207,7 +210,8 @@ static int ctx_init(pf_ctx *ctx, const pf_config *cfg, int device) {
     std::memset(&ctx->tim, 0, sizeof(ctx->tim));
     ctx->tim.t = 0.0;
     ctx->tim.dt = cfg->dt;
-    ctx->tim.pcn = ctx->util_kind == PF_UTIL_CARREAU_YASUDA ? 1 : -1;  // the plug-in's one corrector pass
+    // the plug-ins' one corrector pass
+    ctx->tim.pcn = (ctx->util_kind == PF_UTIL_CARREAU_YASUDA || ctx->util_kind == PF_UTIL_LES) ? 1 : -1;
     ctx->lasterr = 1e99;
     ctx->newdt_i = 0;
     ctx->vel_nu = 1.0;
@@ -259,11 +263,17 @@ extern "C" int pf_ctx_reconfigure(pf_ctx *ctx, const pf_config *cfg) {
     // tim_precompute (timestep.f90:29-40)
     std::memset(&ctx->tim, 0, sizeof(ctx->tim));
     ctx->tim.dt = cfg->dt;
-    ctx->tim.pcn = ctx->util_kind == PF_UTIL_CARREAU_YASUDA ? 1 : -1;  // the plug-in's one corrector pass
+    // the plug-ins' one corrector pass
+    ctx->tim.pcn = (ctx->util_kind == PF_UTIL_CARREAU_YASUDA || ctx->util_kind == PF_UTIL_LES) ? 1 : -1;
     ctx->lasterr = 1e99;
     ctx->newdt_i = 0;
     ctx->vel_nu = 1.0;
     PF_CUDA(cudaMemsetAsync(ctx->dsc, 0, sizeof(DevScalars), ctx->stream));
+    if (ctx->util_kind == PF_UTIL_LES) {  // its filter widths depend on alpha
+        double p[8];
+        std::memcpy(p, ctx->util_par, sizeof(p));
+        PF_TRY(pf_util_set(ctx, PF_UTIL_LES, p, 4));
+    }
     return PF_OK;
 }
 
@@ -288,6 +298,25 @@ extern "C" int pf_ctx_set_stream(pf_ctx *ctx, void *stream) {
         PF_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
         ctx->own_stream = true;
     }
+    return PF_OK;
+}
+
+extern "C" int pf_ctx_set_tuning(pf_ctx *ctx, const pf_tuning *t) {
+    PF_ARG(ctx && t, "pf_ctx_set_tuning: null argument");
+    PF_ARG(t->ld_solver == PF_LD_AUTO || t->ld_solver == PF_LD_STREAMED || t->ld_solver == PF_LD_REBUILT,
+           "pf_ctx_set_tuning: bad ld_solver");
+    PF_TRY(pf_nl_tiles_check(ctx, t));
+    if (std::memcmp(&ctx->tune, t, sizeof(pf_tuning)) == 0) return PF_OK;
+    PF_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->tune = *t;
+    pf_graphs_reset(ctx);
+    ctx->matrices_gen++;  // batches holding this pipe rebuild their launches
+    return PF_OK;
+}
+
+extern "C" int pf_ctx_get_tuning(const pf_ctx *ctx, pf_tuning *t) {
+    PF_ARG(ctx && t, "pf_ctx_get_tuning: null argument");
+    *t = ctx->tune;
     return PF_OK;
 }
 

@@ -87,6 +87,32 @@ struct HostMesh {
 };
 int pf_build_mesh(int N, const double *custom_r, HostMesh &hm);
 
+// Entry A(r, c), |r - c| <= KL, 0 <= r, c < N, of the system c1 I + c2 Lap(PM)
+// for mode (k, m) with the axis-parity first row dr0(:, 1-S) and the wall row
+// dr1(:, BC) (timestep.f90:46-90).  Every product and sum is rounded
+// explicitly (no contraction into fma), so every kernel that assembles an
+// entry gets the same bits: the factorisation (k_lu_factor) and the fused
+// Helmholtz solve that rebuilds its factors on chip.  The matrices of (k, m)
+// and (-k, m) are bitwise equal.
+__device__ __forceinline__ double lumesh_entry(const DevMesh &dm, int N, int Mp, double alpha, int PM, int BC,
+                                               double c1, double c2, int k, int m, int S, int r, int c) {
+    if (r == 0) return dm.dr0[(1 - S) * (PF_KL + 1) + c];
+    if (r == N - 1) return dm.dr1[BC * (PF_KL + 1) + (c - (N - 1 - PF_KL))];
+    double v = __dmul_rn(c2, dm.radLap[(PF_KL + r - c) * N + c]);
+    if (r == c) {
+        const double r2m = dm.rp[1 * N + c];
+        // d = -m^2 Mp^2 / r^2 - alpha^2 k^2, and -1/r^2 - 2 PM m Mp / r^2 for u+-
+        const double t1 = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(r2m, (double)Mp), (double)m), (double)Mp), (double)m);
+        const double t2 = __dmul_rn(__dmul_rn(__dmul_rn(alpha, (double)k), alpha), (double)k);
+        double d = __dsub_rn(-t1, t2);
+        if (PM != 0)
+            d = __dsub_rn(__dsub_rn(d, r2m),
+                          __dmul_rn(__dmul_rn(__dmul_rn(2.0 * PM, (double)Mp), (double)m), r2m));
+        v = __dadd_rn(__dadd_rn(v, __dmul_rn(c2, d)), c1);
+    }
+    return v;
+}
+
 // Device scalars of one context.
 struct DevScalars {
     double Pr0;                      // vel_Pr0
@@ -157,7 +183,10 @@ struct pf_ctx {
     pf_mesh Ltp, Ltm, Ltz;
     bool LNp_set, matrices_ready;
     bool custom_mesh;  // built from a caller-supplied radial mesh
-    unsigned long long matrices_gen;  // bumped by every vel_matrices
+    unsigned long long matrices_gen;  // bumped by every vel_matrices and tuning change
+    pf_tuning tune;      // launch choices (zero = built-in)
+    int last_status;     // corrector check of the last batched step (PF_OK or the abort)
+    std::string last_error;  // its message
     double vel_nu;
     double *U;           // influence solutions [(c*N + n)*Hp + nh], c=0..5
     double *Ainv;        // inverted 4x4 [(i*4+j)*Hp + nh] == A(i+1,j+1,nh)
@@ -180,6 +209,7 @@ struct pf_ctx {
     pf_util_fn util_cb;
     void *util_user;
     double *util_diag_d;
+    double *util_tab;    // per-radial-point tables of a plug-in (LES filter widths)
     unsigned long long util_evals;  // plug-in evaluations since pf_util_set
     unsigned long long *cflmax;  // 3*N CFL maxima of the last fused transform
     bool cfl_fused;              // cflmax is current (else use vel_r/t/z)
@@ -312,6 +342,7 @@ int pf_launch_phys2coll(pf_ctx *ctx, int ncomp, const double *const *src,
 int pf_launch_maxtstep(pf_ctx *ctx, double *dt3);
 int pf_norm_host(pf_ctx *ctx, const double2 *a, double *E, double *Ek, double *Em);
 bool pf_nl_fused_supported(const pf_ctx *ctx);
+int pf_nl_tiles_check(const pf_ctx *ctx, const pf_tuning *t);
 bool pf_util_active(const pf_ctx *ctx);
 int pf_util_run(pf_ctx *ctx, int flag);
 

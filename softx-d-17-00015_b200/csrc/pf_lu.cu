@@ -21,17 +21,16 @@ __global__ void k_lu_factor(double *__restrict__ lu, unsigned char *__restrict__
     const int N = g.N, Hp = g.Hp;
     int k, m;
     mode_km(nh, g.K, k, m);
+    const int S = (m * g.Mp + abs(PM)) % 2;  // axis parity (timestep.f90:82)
     for (int col = 0; col < N; ++col) {
         for (int row = 0; row < KL; ++row) LU(row, col) = 0.0;
-        for (int r2 = 0; r2 < NBAND; ++r2) LU(KL + r2, col) = c2 * dm.radLap[r2 * N + col];
-        const double r2m = dm.rp[1 * N + col];
-        double d = -(r2m * g.Mp * m * g.Mp * m) - g.alpha * k * g.alpha * k;
-        if (PM != 0) d = d - r2m - 2.0 * PM * g.Mp * m * r2m;
-        LU(2 * KL, col) = LU(2 * KL, col) + c2 * d + c1;
+        for (int r2 = 0; r2 < NBAND; ++r2) {  // A(col + r2 - KL, col)
+            const int row = col + r2 - KL;
+            LU(KL + r2, col) = (row >= 0 && row < N)
+                                   ? lumesh_entry(dm, N, g.Mp, g.alpha, PM, BC, c1, c2, k, m, S, row, col)
+                                   : __dmul_rn(c2, dm.radLap[r2 * N + col]);
+        }
     }
-    const int S = (m * g.Mp + abs(PM)) % 2;  // axis parity (timestep.f90:82)
-    for (int j = 1; j <= KL + 1; ++j) LU(2 * KL + 1 - j, j - 1) = dm.dr0[(1 - S) * (KL + 1) + (j - 1)];
-    for (int j = N - KL; j <= N; ++j) LU(2 * KL + N - j, j - 1) = dm.dr1[BC * (KL + 1) + (KL - N + j)];
     if (BC == 1 && k == 0 && m == 0) return;  // singular Neumann mean mode: skipped
     // dgbtf2: A(r,c) lives at band row KV + r - c
     int ju = 0;

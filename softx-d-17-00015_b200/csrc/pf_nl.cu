@@ -33,6 +33,8 @@ struct NLArgs {
     const void *twz, *twt;    // twiddle tables, compute type
     int MC, ZC;               // z-pass columns and theta-pass rows per block
     double *mpart;            // FP64 mean-mode partial sums [ceil(H/32)][N][3]
+    float2 *curlf;            // mixed precision: curl(u) in FP32, [(c*N + n)*Hp + nh], made by the
+                              // mean-mode pass before the z pass reads it (null in FP64)
 };
 
 template <typename C> __device__ __forceinline__ C to_c(double2 v);
@@ -91,21 +93,30 @@ __device__ __forceinline__ void nl_zinv_body(const NLArgs &a, int bx, int by, in
     const int comp = bz, n = by, m0 = bx * MC;
     const int mc = min(MC, g.M - m0);
     fft4_tables<ZL>(tw, tw2, twz);
+    // curl(u) of the mixed-precision path was formed once by the mean-mode
+    // pass; else each input is formed here (u, or curl(u) from 9-row stencils)
+    const float2 *__restrict__ cf = (a.curlf && comp >= 3) ? a.curlf + (size_t)((comp - 3) * g.N + n) * g.Hp : nullptr;
+    auto input = [&](int nh, int k, int m) -> C {
+        if constexpr (sizeof(C) == 8) {
+            if (cf) return cf[nh];
+        }
+        return to_c<C>(nl_input(a, comp, n, nh, k, m));
+    };
     for (int idx = threadIdx.x; idx < mc * ZL; idx += blockDim.x) {
         const int c = idx / ZL, j = idx - c * ZL;
         const int m = m0 + c;
-        double2 v = make_double2(0.0, 0.0);
+        C v = CTraits<C>::make(0, 0);
         if (m == 0) {
-            if (j < K) v = nl_input(a, comp, n, j, j, 0);
+            if (j < K) v = input(j, j, 0);
             else if (j >= 2 * K + 1) {
-                v = nl_input(a, comp, n, ZL - j, ZL - j, 0);
+                v = input(ZL - j, ZL - j, 0);
                 v.y = -v.y;
             }
         } else {
             const int kk = j < K ? j : (j >= 2 * K + 1 ? j - ZL : K);
-            if (kk < K) v = nl_input(a, comp, n, m * (2 * K - 1) + kk, kk, m);
+            if (kk < K) v = input(m * (2 * K - 1) + kk, kk, m);
         }
-        rows[c * RS + j] = to_c<C>(v);
+        rows[c * RS + j] = v;
     }
     __syncthreads();
     FR::template run<+1>(rows, mc, tw, tw2);
@@ -337,21 +348,52 @@ template <typename C> struct NLTiles {
     int MC, ZC;
     size_t zsm, tsm;
 };
-template <typename C> static NLTiles<C> nl_tiles(const Geo &g) {
+static constexpr size_t NL_TILE_MAX_SMEM = 100 * 1024;  // largest tile a tuning may choose
+
+template <typename C> static size_t theta_smem(int Th, int ZC) {
+    return (size_t)(rows_elems<C>(Th, 3 * ZC) + rows_elems<C>(Th, 3 * ZC / 2)) * sizeof(C);
+}
+
+// Tiles of the three transform passes: the tuning's choice where it set one,
+// else the built-in rule.
+template <typename C> static NLTiles<C> nl_tiles(const Geo &g, const pf_tuning &tu) {
     const size_t cs = sizeof(C);
     NLTiles<C> t;
-    // FP32: z-pass tiles up to 32 KB and theta tiles of up to 16 z rows
-    // (measured 4.73 -> 4.59 ms per 64-pipe batch step with the kernels'
+    // built-in: FP32 z-pass tiles up to 32 KB and theta tiles of up to 16 z
+    // rows (measured 4.73 -> 4.59 ms per 64-pipe batch step with the kernels'
     // five-to-six-block launch bounds); FP64: up to 64 KB and 8 rows
     const bool f32 = cs == 8;
-    t.MC = g.M;
-    while (t.MC > 1 && (size_t)rows_elems<C>(g.Z, t.MC) * cs > (f32 ? 32 : 64) * 1024) --t.MC;
+    if (tu.nl_mc > 0) {
+        t.MC = std::min(tu.nl_mc, g.M);
+    } else {
+        t.MC = g.M;
+        while (t.MC > 1 && (size_t)rows_elems<C>(g.Z, t.MC) * cs > (f32 ? 32 : 64) * 1024) --t.MC;
+    }
     t.zsm = (size_t)rows_elems<C>(g.Z, t.MC) * cs;
-    t.ZC = f32 ? 16 : 8;
-    while (t.ZC > 2 && (size_t)(rows_elems<C>(g.Th, 3 * t.ZC) + rows_elems<C>(g.Th, 3 * t.ZC / 2)) * cs > 64 * 1024)
-        t.ZC -= 2;
-    t.tsm = (size_t)(rows_elems<C>(g.Th, 3 * t.ZC) + rows_elems<C>(g.Th, 3 * t.ZC / 2)) * cs;
+    if (tu.nl_zc > 0) {
+        t.ZC = tu.nl_zc;
+    } else {
+        t.ZC = f32 ? 16 : 8;
+        while (t.ZC > 2 && theta_smem<C>(g.Th, t.ZC) > 64 * 1024) t.ZC -= 2;
+    }
+    t.tsm = theta_smem<C>(g.Th, t.ZC);
     return t;
+}
+
+// A tuning's tiles must be even-rowed and fit the shared-memory cap.
+int pf_nl_tiles_check(const pf_ctx *ctx, const pf_tuning *tu) {
+    PF_ARG(tu->nl_mc >= 0 && tu->nl_zc >= 0 && tu->nl_zc <= 32 && tu->nl_zc % 2 == 0,
+           "pf_ctx_set_tuning: nl_mc >= 0, nl_zc even in 0..32");
+    if (!pf_nl_fused_supported(ctx)) return PF_OK;
+    const bool mixed = ctx->cfg.precision == PF_PREC_MIXED;
+    const size_t zsm = mixed ? nl_tiles<float2>(ctx->g, *tu).zsm : nl_tiles<double2>(ctx->g, *tu).zsm;
+    const size_t tsm = mixed ? nl_tiles<float2>(ctx->g, *tu).tsm : nl_tiles<double2>(ctx->g, *tu).tsm;
+    if (zsm > NL_TILE_MAX_SMEM || tsm > NL_TILE_MAX_SMEM) {
+        pf_set_error("pf_ctx_set_tuning: transform tiles need %zu / %zu bytes of shared memory (cap %zu)", zsm, tsm,
+                     NL_TILE_MAX_SMEM);
+        return PF_ERR_ARG;
+    }
+    return PF_OK;
 }
 
 // The fused-transform arguments of one pipe in its current pointer state.
@@ -369,14 +411,16 @@ static NLArgs make_nl_args(pf_ctx *ctx) {
     a.T = ctx->T;
     a.mpart = ctx->mpart;
     const bool mixed = ctx->cfg.precision == PF_PREC_MIXED;
+    // FP32 transforms use the first 6*N*M*Z float2 of T; the curl fields follow
+    a.curlf = mixed ? reinterpret_cast<float2 *>(ctx->T) + (size_t)6 * ctx->g.N * ctx->g.M * ctx->g.Z : nullptr;
     a.twz = mixed ? (const void *)ctx->twZf : (const void *)ctx->twZ;
     a.twt = mixed ? (const void *)ctx->twTf : (const void *)ctx->twT;
     if (mixed) {
-        const NLTiles<float2> t = nl_tiles<float2>(ctx->g);
+        const NLTiles<float2> t = nl_tiles<float2>(ctx->g, ctx->tune);
         a.MC = t.MC;
         a.ZC = t.ZC;
     } else {
-        const NLTiles<double2> t = nl_tiles<double2>(ctx->g);
+        const NLTiles<double2> t = nl_tiles<double2>(ctx->g, ctx->tune);
         a.MC = t.MC;
         a.ZC = t.ZC;
     }
@@ -394,7 +438,7 @@ template <typename K> static int raise_smem(K kernel, size_t bytes, size_t &cur)
 template <typename C>
 static int launch_nl(pf_ctx *ctx, const NLArgs &a) {
     const Geo &g = ctx->g;
-    const NLTiles<C> t = nl_tiles<C>(g);
+    const NLTiles<C> t = nl_tiles<C>(g, ctx->tune);
     const dim3 gz((g.M + t.MC - 1) / t.MC, g.N, 6), gt((g.Z + t.ZC - 1) / t.ZC, g.N), gf((g.M + t.MC - 1) / t.MC, g.N, 3);
     switch (g.Z) {
 #define PF_CASE(L)                                                    \
@@ -448,17 +492,22 @@ __global__ void k_nl_mean64_fin(NLArgs a);
 static int mean_attrs();
 static size_t mean_smem(int N);
 
-// vel_transform + vel_nonlinear in three launches (five in mixed precision);
-// CFL maxima per radial point are left in ctx->cflmax.
+// vel_transform + vel_nonlinear in three launches (five in mixed precision:
+// first the FP64 mean-mode sums, which also leave curl(u) in FP32 for the z
+// pass, last their reduction into the k=m=0 coefficients); CFL maxima per
+// radial point are left in ctx->cflmax.
 int pf_launch_nl_fused(pf_ctx *ctx) {
     const NLArgs a = make_nl_args(ctx);
     if (ctx->cfg.precision == PF_PREC_MIXED) {
+        {
+            ProfScope ps_(ctx, PF_K_ZINV);
+            PF_TRY(mean_attrs());
+            k_nl_mean64_part<<<(ctx->g.H + 31) / 32, MEAN_THREADS, mean_smem(ctx->g.N), ctx->stream>>>(a);
+        }
+        PF_LAUNCHED(ctx);
         PF_TRY(launch_nl<float2>(ctx, a));
         {
             ProfScope ps_(ctx, PF_K_ZFWD);
-            PF_TRY(mean_attrs());
-            k_nl_mean64_part<<<(ctx->g.H + 31) / 32, MEAN_THREADS, mean_smem(ctx->g.N), ctx->stream>>>(a);
-            PF_LAUNCHED(ctx);
             k_nl_mean64_fin<<<(ctx->g.N + 3) / 4, 128, 0, ctx->stream>>>(a);
         }
         PF_LAUNCHED(ctx);
@@ -518,6 +567,12 @@ __device__ __forceinline__ void nl_mean64_part_body(const NLArgs &a, int chunk) 
             const double2 cr = make_double2(-uz.y * m1r1 + ut.y * k1a1, uz.x * m1r1 - ut.x * k1a1);
             const double2 ct = make_double2(-ur.y * k1a1 - dz.x, ur.x * k1a1 - dz.y);
             const double2 cz = make_double2(ut.x * rm1 + dt.x + ur.y * m1r1, ut.y * rm1 + dt.y - ur.x * m1r1);
+            if (a.curlf) {  // the z pass's FP32 inputs of the curl components
+                const size_t at = (size_t)n * Hp + nh, fs = (size_t)N * Hp;
+                a.curlf[at] = make_float2((float)cr.x, (float)cr.y);
+                a.curlf[fs + at] = make_float2((float)ct.x, (float)ct.y);
+                a.curlf[2 * fs + at] = make_float2((float)cz.x, (float)cz.y);
+            }
             const double w = (nh == 0) ? 1.0 : 2.0;
             auto dot = [&](double2 f, double2 h) { return nh == 0 ? f.x * h.x : f.x * h.x + f.y * h.y; };
             s0 = w * (dot(ut, cz) - dot(uz, ct));
@@ -687,7 +742,7 @@ template <typename T> static int upload(T **d, const std::vector<T> &h) {
 
 static bool is_mixed(const pf_ctx *c) { return c->cfg.precision == PF_PREC_MIXED; }
 
-template <typename C> static NLTiles<C> tiles_of(const Geo &g) { return nl_tiles<C>(g); }
+template <typename C> static NLTiles<C> tiles_of(const pf_ctx *c) { return nl_tiles<C>(c->g, c->tune); }
 
 // blocks of stage st for the pipes of one (length, precision) group
 template <typename C>
@@ -696,7 +751,7 @@ static void nlb_group_map(int st, int L, bool mixed, pf_ctx *const *pipes, int n
     for (int i = 0; i < n; ++i) {
         const Geo &g = pipes[i]->g;
         if ((st == 1 ? g.Th : g.Z) != L || is_mixed(pipes[i]) != mixed) continue;
-        const NLTiles<C> t = tiles_of<C>(g);
+        const NLTiles<C> t = tiles_of<C>(pipes[i]);
         int nb = 0;
         if (st == 0) nb = ((g.M + t.MC - 1) / t.MC) * g.N * 6;
         if (st == 1) nb = ((g.Z + t.ZC - 1) / t.ZC) * g.N;
@@ -834,20 +889,24 @@ static int nlb_stage(pf_nl_batch *b, int stage, const NLArgs *args, cudaStream_t
 int pf_nl_batch_launch(pf_nl_batch *b, int state, cudaStream_t st, pf_stage_prof *prof, unsigned long long *nk) {
     const NLArgs *args = b->d_args[state];
     const int cats[NLB_STAGES] = {PF_K_ZINV, PF_K_THFWD, PF_K_ZFWD};
+    // mixed precision: the FP64 mean-mode sums first; they leave curl(u) in
+    // FP32 for the z pass
+    if (b->nmean > 0) {
+        StageScope ss_(prof, PF_K_ZINV, st);
+        PF_TRY(mean_attrs());
+        k_nl_mean64_part_batch<<<b->nmean, MEAN_THREADS, b->mean_sm, st>>>(args, b->mean_blk);
+        PF_CHECK_LAUNCH();
+        *nk += 1;
+    }
     for (int stage = 0; stage < NLB_STAGES; ++stage) {
         StageScope ss_(prof, cats[stage], st);
         PF_TRY(nlb_stage(b, stage, args, st, nk));
     }
     if (b->nmean > 0) {
-        {
-            StageScope ss_(prof, PF_K_ZFWD, st);
-            PF_TRY(mean_attrs());
-            k_nl_mean64_part_batch<<<b->nmean, MEAN_THREADS, b->mean_sm, st>>>(args, b->mean_blk);
-            PF_CHECK_LAUNCH();
-            k_nl_mean64_fin_batch<<<b->nfin, 128, 0, st>>>(args, b->fin_blk);
-        }
+        StageScope ss_(prof, PF_K_ZFWD, st);
+        k_nl_mean64_fin_batch<<<b->nfin, 128, 0, st>>>(args, b->fin_blk);
         PF_CHECK_LAUNCH();
-        *nk += 2;
+        *nk += 1;
     }
     return PF_OK;
 }

@@ -13,7 +13,10 @@
 //     of free contexts, or created), uploads the initial state, builds the
 //     request's matrices and attaches its context to the batch;
 //   * retires the requests that have taken their steps: final state to host
-//     memory, context detached and returned to the pool.
+//     memory, context detached and returned to the pool;
+//   * fails, alone, a request whose corrector check aborted or whose state
+//     went non-finite (NaN or Inf): it leaves the batch without a result and
+//     the others carry on unchanged; a cancelled request leaves the same way.
 // So requests that arrive while others are on the GPU join the running batch
 // as soon as memory and a slot free up, and their work shares every launch
 // with the others.  A request's arithmetic is exactly the lone-pipe path, so
@@ -45,6 +48,8 @@ struct Request {
     std::vector<double> result;
     pf_ctx *ctx;
     long long passes;
+    int status = PF_OK;  // a failed or cancelled request's error
+    std::string error;
 };
 
 // Device bytes of a context of this shape before one exists, from the
@@ -159,6 +164,21 @@ static int admit_one(pf_server *s, int *status) {
     return 1;
 }
 
+// The request ends without a result: out of the batch, its context back to
+// the pool (the next admission overwrites its state and matrices).
+static int drop(pf_server *s, Request *r, int status, const std::string &why) {
+    if (r->ctx) {
+        PF_TRY(pf_batch_detach(s->batch, r->ctx));
+        s->pool.insert({shape_of(r->cfg), r->ctx});
+        r->ctx = nullptr;
+    }
+    r->status = status;
+    r->error = why;
+    s->finished[r->id] = r;
+    s->fresh_done.push_back(r->id);
+    return PF_OK;
+}
+
 static int retire(pf_server *s, Request *r) {
     r->result.resize(6 * r->nval);
     double *a = r->result.data();
@@ -239,6 +259,8 @@ extern "C" int pf_serve_step(pf_server *s, int *admitted, int *finished) {
             if (st != PF_OK) {  // the request cannot run: report it finished with no result
                 Request *r = s->queue.front();
                 s->queue.pop_front();
+                r->status = st;
+                r->error = pf_last_error();
                 s->finished[r->id] = r;
                 s->fresh_done.push_back(r->id);
                 status = st;
@@ -251,13 +273,17 @@ extern "C" int pf_serve_step(pf_server *s, int *admitted, int *finished) {
     if (!s->active.empty()) {
         long long p = 0;
         const int st = pf_batch_step(s->batch, 1, s->orbit, &p);
-        if (st != PF_OK) status = st;
+        // a corrector abort belongs to its own request, reported below
+        if (st != PF_OK && st != PF_ERR_CONVERGE) status = st;
         s->passes += p;
         s->steps += 1;
         std::vector<Request *> still;
         for (Request *r : s->active) {
             r->done += 1;
-            if (r->done >= r->nsteps) {
+            if (r->ctx->last_status != PF_OK) {
+                PF_TRY(drop(s, r, r->ctx->last_status, r->ctx->last_error));
+                ++nf;
+            } else if (r->done >= r->nsteps) {
                 PF_TRY(retire(s, r));
                 ++nf;
             } else {
@@ -281,9 +307,31 @@ extern "C" int pf_serve_finished(pf_server *s, long long *ids, int cap, int *n) 
     return PF_OK;
 }
 
+extern "C" int pf_serve_cancel(pf_server *s, long long id) {
+    PF_ARG(s, "null server");
+    for (auto it = s->queue.begin(); it != s->queue.end(); ++it)
+        if ((*it)->id == id) {
+            Request *r = *it;
+            s->queue.erase(it);
+            return drop(s, r, PF_ERR_CANCELLED, "request cancelled");
+        }
+    for (size_t i = 0; i < s->active.size(); ++i)
+        if (s->active[i]->id == id) {
+            Request *r = s->active[i];
+            s->active.erase(s->active.begin() + i);
+            return drop(s, r, PF_ERR_CANCELLED, "request cancelled");
+        }
+    if (s->finished.count(id)) {
+        pf_set_error("pf_serve_cancel: request %lld has already finished", id);
+        return PF_ERR_STATE;
+    }
+    pf_set_error("pf_serve_cancel: no request %lld", id);
+    return PF_ERR_ARG;
+}
+
 // The final state of a finished request (reference coll layout); the request
-// is forgotten afterwards.  PF_ERR_STATE if it has not finished, and
-// PF_ERR_ARG if it could not run (its admission failed).
+// is forgotten afterwards.  PF_ERR_STATE if it has not finished; a request
+// that failed or was cancelled returns its own status and message.
 extern "C" int pf_serve_result(pf_server *s, long long id, double *ur_re, double *ur_im, double *ut_re,
                                double *ut_im, double *uz_re, double *uz_im) {
     PF_ARG(s, "null server");
@@ -294,10 +342,12 @@ extern "C" int pf_serve_result(pf_server *s, long long id, double *ur_re, double
     }
     Request *r = it->second;
     s->finished.erase(it);
-    if (r->result.empty()) {
+    if (r->status != PF_OK || r->result.empty()) {
+        const int st = r->status != PF_OK ? r->status : PF_ERR_ARG;
+        pf_set_error("pf_serve_result: request %lld: %s", id,
+                     r->error.empty() ? "could not be admitted" : r->error.c_str());
         delete r;
-        pf_set_error("pf_serve_result: request %lld could not be admitted", id);
-        return PF_ERR_ARG;
+        return st;
     }
     double *dst[6] = {ur_re, ur_im, ut_re, ut_im, uz_re, uz_im};
     for (int k = 0; k < 6; ++k)

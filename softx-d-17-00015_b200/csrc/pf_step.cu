@@ -36,6 +36,7 @@ struct StepArgs {
     const double *pivd;    // LNp pivots as doubles [col*Hp + nh]
     const double *pivld[3];  // LDp/LDm/LDz pivots as doubles
     int ldpiv[3];          // 1 if that Helmholtz factorisation pivoted
+    double ldc1, ldc2;     // Helmholtz coefficients (LDp/LDm/LDz: 1/dt, -implicit nu/Re)
     const double *U, *Ainv, *Ui;
     DevMesh dm;
     Geo g;
@@ -435,8 +436,219 @@ __device__ __forceinline__ void solve_ld_body(const StepArgs &a, int bx) {
         solve_async<false, 192>(lu, nullptr, g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x);
 }
 
+// ------------------------- S4 with the factors rebuilt on chip (no pivoting)
+// For a pipe none of whose Helmholtz factorisations pivoted.  One thread per
+// (system, k >= 0, m): it assembles the band of its mode (lumesh_entry, the
+// bits k_lu_factor assembles) and eliminates it column by column in a 5 x 5
+// register window in dgbtf2's order of operations, while the unit-lower
+// sweep of dgbtrs runs on four right-hand sides at once: the real and
+// imaginary parts of mode (k, m) and of its mirror (-k, m), whose matrix is
+// the same.  The rows U(j, j..j+3) of the upper factor go to shared memory
+// for the back substitution (dtbsv); U(j, j+4) is never updated by the
+// elimination, so it is reassembled instead of stored.  Every factor value
+// and every solve operation is the one k_lu_factor + solve_async perform, so
+// the solutions are bitwise those of the streamed-factor path, but the
+// factors never touch HBM: the launch moves the right-hand sides in and the
+// solutions out (plus the forward results, written and read back once).
+//
+// Shared memory per thread: U rows 4*N doubles and a ring of LDR_D
+// right-hand-side rows (two modes, double2) staged ahead by cp.async.
+static constexpr int LDR_BT = 32;  // items per block
+static constexpr int LDR_D = 8;    // right-hand-side rows in flight per item
+
+__device__ __forceinline__ void cp_async16s(unsigned saddr, const void *gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(gmem) : "memory");
+}
+
+static __host__ __device__ inline size_t ldr_smem(int N) {
+    return (size_t)LDR_BT * (4 * (size_t)N * sizeof(double) + (size_t)LDR_D * 2 * sizeof(double2));
+}
+// tiles of one pipe: 3 systems x ceil(M*K / LDR_BT)
+static __host__ __device__ inline int ldr_tiles(const Geo &g) { return 3 * ((g.M * g.K + LDR_BT - 1) / LDR_BT); }
+
+__device__ __forceinline__ void solve_ld_rebuild_body(const StepArgs &a, int tile) {
+    extern __shared__ __align__(16) double ldr_sm[];
+    const Geo &g = a.g;
+    const int N = g.N, K = g.K;
+    const int nitem = g.M * K;
+    const int per = (nitem + LDR_BT - 1) / LDR_BT;
+    const int sys = tile / per;
+    const int item = (tile - sys * per) * LDR_BT + (int)threadIdx.x;
+    if (item >= nitem) return;  // no block barrier below
+    const int m = item / K, k = item - m * K;
+    const int base = m * (2 * K - 1);
+    const bool twin = m > 0 && k > 0;
+    const int nh = m == 0 ? k : base + k;
+    const int nh2 = twin ? base - k : nh;
+    const int PM = sys == 0 ? 1 : (sys == 1 ? -1 : 0);
+    const int S = (m * g.Mp + abs(PM)) % 2;
+    const double c1 = a.ldc1, c2 = a.ldc2;
+    const DevMesh &dm = a.dm;
+    const size_t Hp = g.Hp;
+    const double2 *__restrict__ rhs = pick3(a.rl, sys);
+    double2 *__restrict__ out = pick3(a.v, sys);
+    double *ur = ldr_sm + threadIdx.x;  // U(j, j+c) at ur[(j*4 + c) * LDR_BT]
+    double2 *ring = reinterpret_cast<double2 *>(ldr_sm + (size_t)4 * N * LDR_BT) + threadIdx.x;
+    const unsigned rbase = (unsigned)__cvta_generic_to_shared(ring);
+    constexpr unsigned RSTEP = 16u * LDR_BT;  // bytes between ring entries
+    auto A = [&](int r, int c) { return lumesh_entry(dm, N, g.Mp, g.alpha, PM, 0, c1, c2, k, m, S, r, c); };
+    // right-hand-side rows enter in order 0, 1, 2, ...; row r sits in slot r % LDR_D
+    int rin = 0;
+    auto issue = [&](void) {
+        if (rin < N) {
+            const unsigned sa = rbase + (unsigned)((rin % LDR_D) * 2) * RSTEP;
+            cp_async16s(sa, rhs + (size_t)rin * Hp + nh);
+            cp_async16s(sa + RSTEP, rhs + (size_t)rin * Hp + nh2);
+        }
+        cp_async_commit();
+        ++rin;
+    };
+#pragma unroll
+    for (int q = 0; q < LDR_D; ++q) issue();
+    cp_async_wait<LDR_D - 5>();  // rows 0..4
+    // forward window: W[i][c] = A(j+i, j+c) as eliminated so far, held in
+    // physical slot [(i+j)%5][(c+j)%5]; right-hand sides w[q][(i+j)%5]
+    double W[5][5];
+    double2 w0[5], w1[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) W[i][c] = (i < N && c < N) ? A(i, c) : 0.0;
+        const bool in = i < N;
+        w0[i] = in ? ring[(size_t)((i % LDR_D) * 2) * LDR_BT] : make_double2(0.0, 0.0);
+        w1[i] = in ? ring[(size_t)((i % LDR_D) * 2 + 1) * LDR_BT] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) issue();
+    double2 *Yj = out;  // forward results y(j) of mode nh, then of nh2 at +(nh2-nh)
+    const ptrdiff_t d2 = (ptrdiff_t)nh2 - (ptrdiff_t)nh;
+    Yj += nh;
+    for (int j0 = 0; j0 < N; j0 += 5) {
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            const int j = j0 + s;
+            if (j < N) {
+                const int km = min(KL, N - 1 - j);
+                // column j of L and row j of U (dgbtf2, no interchange)
+                double L[5];
+                const double piv = W[s % 5][s % 5];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) ur[(size_t)(j * 4 + c) * LDR_BT] = W[s % 5][(c + s) % 5];
+                if (km > 0) {
+                    const double rp = 1.0 / piv;
+#pragma unroll
+                    for (int i = 1; i <= KL; ++i) L[i] = (i <= km) ? W[(i + s) % 5][s % 5] * rp : 0.0;
+#pragma unroll
+                    for (int c = 1; c <= KL; ++c) {
+                        if (c > km) break;
+                        const double y = -W[s % 5][(c + s) % 5];
+#pragma unroll
+                        for (int i = 1; i <= KL; ++i)
+                            if (i <= km) W[(i + s) % 5][(c + s) % 5] = fma(L[i], y, W[(i + s) % 5][(c + s) % 5]);
+                    }
+                    // dgbtrs forward sweep on the four right-hand sides
+                    const double2 b0 = w0[s % 5], b1 = w1[s % 5];
+#pragma unroll
+                    for (int i = 1; i <= KL; ++i)
+                        if (i <= km) {
+                            double2 &x0 = w0[(i + s) % 5], &x1 = w1[(i + s) % 5];
+                            x0.x = fma(-L[i], b0.x, x0.x);
+                            x0.y = fma(-L[i], b0.y, x0.y);
+                            x1.x = fma(-L[i], b1.x, x1.x);
+                            x1.y = fma(-L[i], b1.y, x1.y);
+                        }
+                }
+                Yj[0] = w0[s % 5];
+                if (twin) Yj[d2] = w1[s % 5];
+                Yj += Hp;
+                // the row entering the right-hand-side window: j + 5
+                cp_async_wait<LDR_D - 1>();
+                const bool more = j + 5 < N;
+                const int sl = ((j + 5) % LDR_D) * 2;
+                w0[s % 5] = more ? ring[(size_t)sl * LDR_BT] : make_double2(0.0, 0.0);
+                w1[s % 5] = more ? ring[(size_t)(sl + 1) * LDR_BT] : make_double2(0.0, 0.0);
+                issue();
+                // the window moves one row down and one column right: row j+5
+                // and column j+5 enter with their assembled values
+#pragma unroll
+                for (int c = 0; c < 5; ++c) W[s % 5][(c + s) % 5] = (more && c >= 1) ? A(j + 5, j + c) : 0.0;
+                if (more) W[s % 5][s % 5] = A(j + 5, j + 5);
+#pragma unroll
+                for (int i = 1; i < 5; ++i) W[(i + s) % 5][s % 5] = more ? A(j + i, j + 5) : 0.0;
+            }
+        }
+    }
+    cp_async_wait<0>();
+    // back substitution (dtbsv) on the four right-hand sides; y(j) is read
+    // back through a register queue QY rows ahead
+    constexpr int QY = 4;
+    const double2 *Yr = out + nh;
+    double2 v0[5], v1[5], q0[QY], q1[QY];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        const int r = N - 1 - i;
+        v0[i] = r >= 0 ? __ldcg(Yr + (size_t)r * Hp) : make_double2(0.0, 0.0);
+        v1[i] = (r >= 0 && twin) ? __ldcg(Yr + (size_t)r * Hp + d2) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int q = 0; q < QY; ++q) {
+        const int r = N - 1 - 5 - q;
+        q0[q] = r >= 0 ? __ldcg(Yr + (size_t)r * Hp) : make_double2(0.0, 0.0);
+        q1[q] = (r >= 0 && twin) ? __ldcg(Yr + (size_t)r * Hp + d2) : make_double2(0.0, 0.0);
+    }
+    double2 *Xj = out + nh + (size_t)(N - 1) * Hp;
+    for (int t0 = 0; t0 < N; t0 += 5) {
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            const int t = t0 + s;
+            if (t < N) {
+                const int j = N - 1 - t;
+                // U(j-i, j), i = 0..4
+                double Uc[5];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) Uc[i] = (j - i >= 0) ? ur[(size_t)((j - i) * 4 + i) * LDR_BT] : 0.0;
+                Uc[4] = (j - 4 >= 0) ? A(j - 4, j) : 0.0;
+                double2 x0 = v0[s % 5], x1 = v1[s % 5];
+                // dtbsv skips a column whose right-hand side is exactly zero
+                const bool n0x = x0.x != 0.0, n0y = x0.y != 0.0, n1x = x1.x != 0.0, n1y = x1.y != 0.0;
+                const double u = Uc[0];
+                if (n0x) x0.x = x0.x / u;
+                if (n0y) x0.y = x0.y / u;
+                if (n1x) x1.x = x1.x / u;
+                if (n1y) x1.y = x1.y / u;
+#pragma unroll
+                for (int i = 1; i <= KL; ++i)
+                    if (j - i >= 0) {
+                        double2 &a0 = v0[(i + s) % 5], &a1 = v1[(i + s) % 5];
+                        if (n0x) a0.x = fma(-x0.x, Uc[i], a0.x);
+                        if (n0y) a0.y = fma(-x0.y, Uc[i], a0.y);
+                        if (n1x) a1.x = fma(-x1.x, Uc[i], a1.x);
+                        if (n1y) a1.y = fma(-x1.y, Uc[i], a1.y);
+                    }
+                Xj[0] = x0;
+                if (twin) Xj[d2] = x1;
+                Xj -= Hp;
+                const bool more = j - 5 >= 0;
+                v0[s % 5] = more ? q0[0] : make_double2(0.0, 0.0);
+                v1[s % 5] = more ? q1[0] : make_double2(0.0, 0.0);
+#pragma unroll
+                for (int q = 0; q < QY - 1; ++q) {
+                    q0[q] = q0[q + 1];
+                    q1[q] = q1[q + 1];
+                }
+                const int r = j - 5 - QY;
+                q0[QY - 1] = r >= 0 ? __ldcg(Yr + (size_t)r * Hp) : make_double2(0.0, 0.0);
+                q1[QY - 1] = (r >= 0 && twin) ? __ldcg(Yr + (size_t)r * Hp + d2) : make_double2(0.0, 0.0);
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------------- S5
 __device__ __forceinline__ double sq(double2 a) { return a.x * a.x + a.y * a.y; }
+// max that keeps a NaN (fmax drops it): a state gone non-finite shows as a
+// NaN corrector error instead of a converged one
+__device__ __forceinline__ double nanmax(double a, double b) { return (b > a || b != b) ? b : a; }
 
 __device__ __forceinline__ void step_final_body(const StepArgs &a, int bx) {
     __shared__ double coef[TM][8];        // aR(1..4), aI(1..4) per mode
@@ -548,9 +760,9 @@ __device__ __forceinline__ void step_final_body(const StepArgs &a, int bx) {
                     continue;
                 }
                 if (a.mode == 1) {
-                    err = fmax(err, sq(make_double2(o[q][0].x - ur.x, o[q][0].y - ur.y)));
-                    err = fmax(err, sq(make_double2(o[q][1].x - ut.x, o[q][1].y - ut.y)));
-                    err = fmax(err, sq(make_double2(o[q][2].x - zz.x, o[q][2].y - zz.y)));
+                    err = nanmax(err, sq(make_double2(o[q][0].x - ur.x, o[q][0].y - ur.y)));
+                    err = nanmax(err, sq(make_double2(o[q][1].x - ut.x, o[q][1].y - ut.y)));
+                    err = nanmax(err, sq(make_double2(o[q][2].x - zz.x, o[q][2].y - zz.y)));
                 }
                 u0[at] = ur;
                 u1[at] = ut;
@@ -581,9 +793,9 @@ __device__ __forceinline__ void step_final_body(const StepArgs &a, int bx) {
             const double2 uz = make_double2(zr, 0.0);
             if (a.mode == 1) {
                 const double2 o0 = a.u[0][at], o1 = a.u[1][at], o2 = a.u[2][at];
-                err = fmax(err, sq(make_double2(o0.x - ur.x, o0.y - ur.y)));
-                err = fmax(err, sq(make_double2(o1.x - ut.x, o1.y - ut.y)));
-                err = fmax(err, sq(make_double2(o2.x - uz.x, o2.y - uz.y)));
+                err = nanmax(err, sq(make_double2(o0.x - ur.x, o0.y - ur.y)));
+                err = nanmax(err, sq(make_double2(o1.x - ut.x, o1.y - ut.y)));
+                err = nanmax(err, sq(make_double2(o2.x - uz.x, o2.y - uz.y)));
             }
             a.u[0][at] = ur;
             a.u[1][at] = ut;
@@ -593,12 +805,12 @@ __device__ __forceinline__ void step_final_body(const StepArgs &a, int bx) {
     }
     if (a.mode == 1) {  // one atomic per block: warp maxima, then the block's
         __shared__ double wmax[TM * TR / 32];
-        for (int o = 16; o > 0; o >>= 1) err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
+        for (int o = 16; o > 0; o >>= 1) err = nanmax(err, __shfl_xor_sync(0xffffffffu, err, o));
         if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = err;
         __syncthreads();
         if (threadIdx.x == 0) {
             double e = wmax[0];
-            for (int i = 1; i < TM * TR / 32; ++i) e = fmax(e, wmax[i]);
+            for (int i = 1; i < TM * TR / 32; ++i) e = nanmax(e, wmax[i]);
             atomicMax(&a.sc->dterr2_bits, (unsigned long long)__double_as_longlong(e));
         }
     }
@@ -612,6 +824,7 @@ __global__ void __launch_bounds__(HM *HR, 3) k_step_rhs(StepArgs a) { step_rhs_b
 __global__ void __launch_bounds__(64, 8) k_solve_pnp(StepArgs a) { solve_pnp_body(a, blockIdx.x); }
 __global__ void k_step_proj(StepArgs a) { step_proj_body(a, blockIdx.x, blockIdx.y); }
 __global__ void __launch_bounds__(192, 4) k_solve_ld(StepArgs a) { solve_ld_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(LDR_BT) k_solve_ldr(StepArgs a) { solve_ld_rebuild_body(a, blockIdx.x); }
 __global__ void __launch_bounds__(TM *TR) k_step_final(StepArgs a) { step_final_body(a, blockIdx.x); }
 
 #define PF_BATCH1(NAME, BODY, BOUNDS)                                                          \
@@ -622,6 +835,7 @@ __global__ void __launch_bounds__(TM *TR) k_step_final(StepArgs a) { step_final_
     }
 PF_BATCH1(k_solve_pnp_batch, solve_pnp_body, __launch_bounds__(64, 8))
 PF_BATCH1(k_solve_ld_batch, solve_ld_body, __launch_bounds__(192, 4))
+PF_BATCH1(k_solve_ldr_batch, solve_ld_rebuild_body, __launch_bounds__(LDR_BT))
 PF_BATCH1(k_step_final_batch, step_final_body, __launch_bounds__(TM *TR))
 #undef PF_BATCH1
 
@@ -664,6 +878,8 @@ static StepArgs make_step_args(const pf_ctx *ctx, int corrector) {
         a.pivld[i] = ld[i]->pivd;
         a.ldpiv[i] = ld[i]->pivoted;
     }
+    a.ldc1 = ctx->LDp.c1;
+    a.ldc2 = ctx->LDp.c2;
     a.ldp = ctx->LDp.lu;
     a.ldm = ctx->LDm.lu;
     a.ldz = ctx->LDz.lu;
@@ -685,6 +901,13 @@ static bool any_ld_pivoted(const pf_ctx *ctx) {
     return ctx->LDp.pivoted || ctx->LDm.pivoted || ctx->LDz.pivoted;
 }
 
+// The Helmholtz solves rebuild their factors on chip when the tuning asks
+// for it (PF_LD_REBUILT), no factorisation pivoted and N >= 2 KL + 2; the
+// built-in choice streams them.
+static bool ld_rebuild(const pf_ctx *ctx) {
+    return !any_ld_pivoted(ctx) && ctx->g.N >= 2 * KL + 2 && ctx->tune.ld_solver == PF_LD_REBUILT;
+}
+
 static size_t rhs_smem(int N) { return (size_t)N * HM * sizeof(double2); }
 
 static int step_attrs() {
@@ -696,6 +919,9 @@ static int step_attrs() {
         PF_CUDA(cudaFuncSetAttribute(k_solve_pnp, cudaFuncAttributeMaxDynamicSharedMemorySize, pnp));
         PF_CUDA(cudaFuncSetAttribute(k_solve_ld_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, ld));
         PF_CUDA(cudaFuncSetAttribute(k_solve_pnp_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, pnp));
+        const int ldr = (int)ldr_smem(HR * 8);
+        PF_CUDA(cudaFuncSetAttribute(k_solve_ldr, cudaFuncAttributeMaxDynamicSharedMemorySize, ldr));
+        PF_CUDA(cudaFuncSetAttribute(k_solve_ldr_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, ldr));
         const int rhs = (int)rhs_smem(128);
         PF_CUDA(cudaFuncSetAttribute(k_step_rhs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, rhs));
         PF_CUDA(cudaFuncSetAttribute(k_step_rhs<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, rhs));
@@ -733,7 +959,7 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
     }
     PF_LAUNCHED(ctx);
     {
-        ProfScope ps_(ctx, PF_K_LUSOLVE);
+        ProfScope ps_(ctx, PF_K_PPE);
         k_solve_pnp<<<tiles, 64, (size_t)64 * RING * (KV + 1) * sizeof(double), ctx->stream>>>(a);
     }
     PF_LAUNCHED(ctx);
@@ -744,7 +970,10 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
     PF_LAUNCHED(ctx);
     {
         ProfScope ps_(ctx, PF_K_LUSOLVE);
-        k_solve_ld<<<tiles, 192, (size_t)192 * RING * ldsw * sizeof(double), ctx->stream>>>(a);
+        if (ld_rebuild(ctx))
+            k_solve_ldr<<<ldr_tiles(g), LDR_BT, ldr_smem(g.N), ctx->stream>>>(a);
+        else
+            k_solve_ld<<<tiles, 192, (size_t)192 * RING * ldsw * sizeof(double), ctx->stream>>>(a);
     }
     PF_LAUNCHED(ctx);
     {
@@ -765,6 +994,8 @@ struct pf_step_batch {
     int ntile, nproj, nhalf;
     int2 *ldmap[2];            // 32-mode tiles of the pipes whose Helmholtz factors [0] never / [1] pivot
     int nld[2];
+    int2 *ldrmap;              // tiles of the pipes whose Helmholtz factors are rebuilt on chip
+    int nldr, ldrN;            // their count and largest N
     int maxN;
     bool anypiv;
 };
@@ -777,6 +1008,7 @@ void pf_step_batch_free(pf_step_batch *b) {
     cudaFree(b->half);
     cudaFree(b->ldmap[0]);
     cudaFree(b->ldmap[1]);
+    cudaFree(b->ldrmap);
     cudaFree(b->proj);
     delete b;
 }
@@ -789,7 +1021,8 @@ int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
     b->maxN = 0;
     b->anypiv = false;
     std::vector<StepArgs> h(n);
-    std::vector<int2> tile, proj, half, ldm[2];
+    std::vector<int2> tile, proj, half, ldm[2], ldr;
+    b->ldrN = 0;
     for (int i = 0; i < n; ++i) {
         const Geo &g = pipes[i]->g;
         if (!pf_fused_step_geo_ok(g)) {
@@ -800,7 +1033,12 @@ int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
         b->maxN = std::max(b->maxN, g.N);
         b->anypiv |= any_ld_pivoted(pipes[i]);
         for (int t = 0; t < (int)grid1(g.H, TM); ++t) tile.push_back(make_int2(i, t));
-        for (int t = 0; t < (int)grid1(g.H, TM); ++t) ldm[any_ld_pivoted(pipes[i]) ? 1 : 0].push_back(make_int2(i, t));
+        if (ld_rebuild(pipes[i])) {
+            for (int t = 0; t < ldr_tiles(g); ++t) ldr.push_back(make_int2(i, t));
+            b->ldrN = std::max(b->ldrN, g.N);
+        } else {
+            for (int t = 0; t < (int)grid1(g.H, TM); ++t) ldm[any_ld_pivoted(pipes[i]) ? 1 : 0].push_back(make_int2(i, t));
+        }
         for (int t = 0; t < (int)grid1(g.H, HM); ++t) half.push_back(make_int2(i, t));
         for (int t = 0; t < (int)(grid1(g.H, 128) * grid1(g.N, PR)); ++t) proj.push_back(make_int2(i, t));
     }
@@ -830,6 +1068,14 @@ int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
             pf_set_error("batched step: tile map upload failed");
             return PF_ERR_CUDA;
         }
+    }
+    b->nldr = (int)ldr.size();
+    if (cudaMalloc((void **)&b->ldrmap, std::max<size_t>(1, ldr.size()) * sizeof(int2)) != cudaSuccess ||
+        (!ldr.empty() && cudaMemcpy(b->ldrmap, ldr.data(), ldr.size() * sizeof(int2), cudaMemcpyHostToDevice) !=
+                             cudaSuccess)) {
+        pf_step_batch_free(b);
+        pf_set_error("batched step: tile map upload failed");
+        return PF_ERR_CUDA;
     }
     if (cudaMalloc((void **)&b->half, half.size() * sizeof(int2)) != cudaSuccess ||
         cudaMemcpy(b->half, half.data(), half.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -865,7 +1111,7 @@ int pf_step_batch_launch(pf_step_batch *b, int state, int corrector, cudaStream_
     }
     PF_CHECK_LAUNCH();
     {
-        StageScope ss_(prof, PF_K_LUSOLVE, st);
+        StageScope ss_(prof, PF_K_PPE, st);
         k_solve_pnp_batch<<<b->ntile, 64, (size_t)64 * RING * (KV + 1) * sizeof(double), st>>>(a, b->tile);
     }
     PF_CHECK_LAUNCH();
@@ -882,6 +1128,7 @@ int pf_step_batch_launch(pf_step_batch *b, int state, int corrector, cudaStream_
             if (b->nld[q] > 0)
                 k_solve_ld_batch<<<b->nld[q], 192, (size_t)192 * RING * (q ? KV + 1 : KL + 1) * sizeof(double), st>>>(
                     a, b->ldmap[q]);
+        if (b->nldr > 0) k_solve_ldr_batch<<<b->nldr, LDR_BT, ldr_smem(b->ldrN), st>>>(a, b->ldrmap);
     }
     PF_CHECK_LAUNCH();
     {
@@ -889,6 +1136,6 @@ int pf_step_batch_launch(pf_step_batch *b, int state, int corrector, cudaStream_
         k_step_final_batch<<<b->ntile, TM * TR, 0, st>>>(a, b->tile);
     }
     PF_CHECK_LAUNCH();
-    *nk += 4 + (b->nld[0] > 0) + (b->nld[1] > 0);
+    *nk += 4 + (b->nld[0] > 0) + (b->nld[1] > 0) + (b->nldr > 0);
     return PF_OK;
 }

@@ -263,9 +263,18 @@ static int replay(pf_ctx *ctx, int slot, cudaGraphExec_t g, unsigned long long n
     return PF_OK;
 }
 
+// A plug-in whose hook is device work only, queued on the context's stream
+// (the Coriolis and Carreau-Yasuda terms), rides in the step graphs; a host
+// callback, and LES (it reads max nu_t back to decide on new matrices before
+// its terms), keep the step eager.
+static bool util_graphable(const pf_ctx *ctx) {
+    return ctx->util_cb == nullptr && (ctx->util_kind == PF_UTIL_NONE || ctx->util_kind == PF_UTIL_CORIOLIS ||
+                                       ctx->util_kind == PF_UTIL_CARREAU_YASUDA);
+}
+
 static bool graphs_ok(const pf_ctx *ctx) {
     return ctx->use_graphs && ctx->cfg.dt > 0.0 && pf_nl_fused_supported(ctx) && fused_step_ok(ctx) &&
-           !pf_util_active(ctx);
+           util_graphable(ctx);
 }
 
 // vel_transform + vel_nonlinear + var_null(2) of the main loop (main.f90:21-23,
@@ -290,11 +299,14 @@ extern "C" int pf_timestep(pf_ctx *ctx, int *ncorr) {
     if (graphs_ok(ctx) && ctx->graph_warm) {
         const int p = ctx->parity;
         if (!ctx->g_main[p]) {
+            // with a built-in plug-in its var_null(2) terms follow each
+            // nonlinear evaluation inside the graph (its var_null(1) does
+            // nothing on the device)
             PF_TRY(capture(ctx, p, &ctx->g_main[p], &ctx->g_main_n[p], [&]() {
                 PF_TRY(pf_vel_imposesym(ctx));
-                PF_TRY(transform_nonlinear(ctx));
+                PF_TRY(main_nonlinear(ctx));
                 PF_TRY(pf_vel_step_fused(ctx, 0));
-                PF_TRY(transform_nonlinear(ctx));
+                PF_TRY(main_nonlinear(ctx));
                 return pf_vel_step_fused(ctx, 1);
             }));
             // capture swapped the host pointers; the replay below does it for real
@@ -304,7 +316,7 @@ extern "C" int pf_timestep(pf_ctx *ctx, int *ncorr) {
         PF_TRY(replay(ctx, p, ctx->g_main[p], ctx->g_main_n[p]));
         for (int i = 0; i < 3; ++i) std::swap(ctx->vel[i].d, ctx->prev[i].d);
         ctx->parity = p ^ 1;
-        ctx->cfl_fused = true;
+        ctx->cfl_fused = !pf_util_active(ctx);  // the plug-in path materialises vel_r..vel_z instead
         ctx->tim.it = 1;
         for (;;) {
             PF_TRY(read_dterr(ctx));
@@ -315,7 +327,7 @@ extern "C" int pf_timestep(pf_ctx *ctx, int *ncorr) {
             const int q = ctx->parity;
             if (!ctx->g_corr[q])
                 PF_TRY(capture(ctx, 2 + q, &ctx->g_corr[q], &ctx->g_corr_n[q], [&]() {
-                    PF_TRY(transform_nonlinear(ctx));
+                    PF_TRY(main_nonlinear(ctx));
                     return pf_vel_step_fused(ctx, 1);
                 }));
             PF_TRY(replay(ctx, 2 + q, ctx->g_corr[q], ctx->g_corr_n[q]));

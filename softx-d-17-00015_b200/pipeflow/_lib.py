@@ -18,12 +18,14 @@ PF_ERR_NOMEM = -4
 PF_ERR_STATE = -5
 PF_ERR_CONVERGE = -6
 PF_ERR_NODEVICE = -7
+PF_ERR_CANCELLED = -8
 PF_PREC_FP64 = 0
 PF_PREC_MIXED = 1
 PF_IO_TIME_FROM_FILE = 1
 PF_UTIL_NONE = 0
 PF_UTIL_CORIOLIS = 1
 PF_UTIL_CARREAU_YASUDA = 2
+PF_UTIL_LES = 3
 UTIL_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_void_p)
 KL = 4
 
@@ -50,6 +52,15 @@ class pf_tim_state(C.Structure):
     ]
 
 
+PF_LD_AUTO = 0
+PF_LD_STREAMED = 1
+PF_LD_REBUILT = 2
+
+
+class pf_tuning(C.Structure):
+    _fields_ = [("ld_solver", C.c_int), ("nl_mc", C.c_int), ("nl_zc", C.c_int)]
+
+
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
 D = C.c_double
@@ -65,6 +76,8 @@ _SIGS = {
     "pf_ctx_destroy": [P],
     "pf_ctx_reconfigure": [P, C.POINTER(pf_config)],
     "pf_ctx_set_stream": [P, P],
+    "pf_ctx_set_tuning": [P, C.POINTER(pf_tuning)],
+    "pf_ctx_get_tuning": [P, C.POINTER(pf_tuning)],
     "pf_ctx_sync": [P],
     "pf_ctx_dims": [P, IP, IP, IP, IP],
     "pf_ctx_device_bytes": [P, C.POINTER(C.c_ulonglong)],
@@ -158,6 +171,7 @@ _SIGS = {
     "pf_batch_io_sync": [P],
     "pf_batch_prof_enable": [P, I],
     "pf_batch_prof_read": [P, I, DP, C.POINTER(C.c_ulonglong)],
+    "pf_batch_prof_read_staged": [P, I, DP, C.POINTER(C.c_ulonglong)],
     "pf_batch_launches": [P, C.POINTER(C.c_ulonglong)],
     "pf_batch_size": [P, C.POINTER(I)],
     "pf_batch_attach": [P, P],
@@ -169,6 +183,7 @@ _SIGS = {
     "pf_serve_step": [P, C.POINTER(I), C.POINTER(I)],
     "pf_serve_finished": [P, C.POINTER(C.c_longlong), I, C.POINTER(I)],
     "pf_serve_result": [P, C.c_longlong, DP, DP, DP, DP, DP, DP],
+    "pf_serve_cancel": [P, C.c_longlong],
     "pf_serve_stats": [P, C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(C.c_ulonglong),
                        C.POINTER(C.c_longlong)],
     "pf_serve_batch": [P, PP],

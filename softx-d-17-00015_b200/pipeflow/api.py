@@ -234,6 +234,18 @@ class Pipe:
         except Exception:
             pass
 
+    # ---------------- launch choices ----------------
+    def set_tuning(self, ld_solver: int = L.PF_LD_AUTO, nl_mc: int = 0, nl_zc: int = 0):
+        """Launch choices of the fused step (pf_ctx_set_tuning); every choice
+        gives the same numbers bit for bit, only the speed differs."""
+        t = L.pf_tuning(int(ld_solver), int(nl_mc), int(nl_zc))
+        _check(self.lib.pf_ctx_set_tuning(self.ctx, C.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = L.pf_tuning()
+        _check(self.lib.pf_ctx_get_tuning(self.ctx, C.byref(t)))
+        return {"ld_solver": t.ld_solver, "nl_mc": t.nl_mc, "nl_zc": t.nl_zc}
+
     # ---------------- fields ----------------
     def coll(self, re=None, im=None) -> Coll:
         c = Coll(self)
@@ -442,6 +454,13 @@ class Pipe:
         _check(self.lib.pf_vel_get_scalars(self.ctx, C.byref(p), None))
         return p.value
 
+    @property
+    def vel_nu(self) -> float:
+        """The reference viscosity of the implicit operator (velocity.f90:26)."""
+        p = C.c_double()
+        _check(self.lib.pf_vel_get_scalars(self.ctx, None, C.byref(p)))
+        return p.value
+
     def influence(self):
         """U (6, H, N) and the inverted A (H, 4, 4) of vel_adjPPE(0)."""
         U = np.empty((6, self.H, self.N))
@@ -507,7 +526,7 @@ class Pipe:
 
     # ---------------- instrumentation ----------------
     KERNEL_CATEGORIES = ("zinv", "thinv", "thfwd", "zfwd", "lusolve", "stencil", "ew", "infl",
-                         "factor", "step")
+                         "factor", "step", "ppe")
 
     def launches(self) -> int:
         n = C.c_ulonglong()
@@ -629,12 +648,15 @@ class Batch:
             mask = sum(1 << cats.index(n) for n in on)
         _check(self.lib.pf_batch_prof_enable(self.h, mask))
 
-    def prof_read(self):
-        """{category: (total ms, launches)} summed over the pipes."""
+    def prof_read(self, staged_only=False):
+        """{category: (total ms, launches)} summed over the pipes; with
+        staged_only, the spans of the stage-batched launches alone (each
+        covers every pipe), without per-pipe launches."""
+        fn = self.lib.pf_batch_prof_read_staged if staged_only else self.lib.pf_batch_prof_read
         out = {}
         for i, name in enumerate(Pipe.KERNEL_CATEGORIES):
             ms, n = C.c_double(), C.c_ulonglong()
-            _check(self.lib.pf_batch_prof_read(self.h, i, C.byref(ms), C.byref(n)))
+            _check(fn(self.h, i, C.byref(ms), C.byref(n)))
             out[name] = (ms.value, n.value)
         return out
 
@@ -704,8 +726,15 @@ class Server:
         _check(self.lib.pf_serve_finished(self.h, ids, cap, C.byref(n)))
         return [ids[i] for i in range(n.value)]
 
+    def cancel(self, rid: int):
+        """Withdraw a queued or running request (pf_serve_cancel); it is
+        reported finished and its result() raises PF_ERR_CANCELLED."""
+        _check(self.lib.pf_serve_cancel(self.h, int(rid)))
+
     def result(self, rid: int):
-        """Final state as Pipe.get_state returns it; the request is forgotten."""
+        """Final state as Pipe.get_state returns it; the request is forgotten.
+        A request that failed (corrector abort, non-finite state, admission)
+        or was cancelled raises PipeflowError with its own status."""
         H, N = self._shape.pop(rid)
         out = [np.empty((H, N), dtype=np.float64) for _ in range(6)]
         _check(self.lib.pf_serve_result(self.h, int(rid), *[_dp(a) for a in out]))

@@ -1,0 +1,188 @@
+"""Autotuner of the fused timestep's launch choices.
+
+No counterpart in the reference: its only tuning is FFTW's own plan search
+(FFTW_PATIENT, transform.fftw3.f90:36-57), which picks radices per transform
+length.  Here the choices are those pf_ctx_set_tuning exposes:
+
+  ld_solver  the Helmholtz banded solves stream the stored LU factors from
+             HBM (PF_LD_STREAMED, the built-in choice) or rebuild them on
+             chip (PF_LD_REBUILT, for factorisations that did not pivot);
+  nl_mc      columns (azimuthal modes m) per block of the z transform passes;
+  nl_zc      z rows per block of the theta pass (two rows per complex FFT).
+
+Every choice gives the same numbers bit for bit, so the tuner only times
+them.  It times timesteps in the steporbit form (exactly one corrector per
+step, so every candidate does the same work), by coordinate descent: the
+solver first, then the z tile, then the theta tile, each with the others
+held.  A pipe is tuned on its own; a batch is tuned shape by shape (pipes of
+one (N, K, M, Mp, precision) share a choice) while the whole batch steps,
+since the kernels of different shapes share the GPU.  Choices are cached in
+a JSON file (PIPEFLOW_TUNE_CACHE, default ~/.cache/pipeflow_b200/tuning.json)
+keyed by the pipe shape, or by the batch's shape multiset.
+
+The tuner advances the flow while it times; it restores every pipe's state
+and time-stepping counters afterwards.
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+from pathlib import Path
+
+from . import _lib as L
+from .api import PipeflowError
+
+ZC_CANDIDATES = (0, 4, 8, 16, 32)
+
+
+def _mc_candidates(M: int):
+    out = {0, M}
+    for d in (2, 3, 4, 6, 8):
+        out.add(max(1, -(-M // d)))
+    return sorted(out)
+
+
+def shape_of(pipe) -> tuple:
+    return (pipe.N, pipe.K, pipe.M, pipe.Mp, int(getattr(pipe.cfg, "precision", 0)))
+
+
+def _shape_key(shape) -> str:
+    N, K, M, Mp, prec = shape
+    return f"N{N}K{K}M{M}Mp{Mp}{'mixed' if prec == L.PF_PREC_MIXED else 'fp64'}"
+
+
+def default_cache_path() -> Path:
+    env = os.environ.get("PIPEFLOW_TUNE_CACHE")
+    if env:
+        return Path(env)
+    return Path.home() / ".cache" / "pipeflow_b200" / "tuning.json"
+
+
+class _Snapshot:
+    """Host copies of pipes' states and time-stepping counters."""
+
+    def __init__(self, pipes):
+        self.items = [(p, p.get_state(), p.tim) for p in pipes]
+
+    def restore(self):
+        for p, st, tim in self.items:
+            p.set_state(*st)
+            p.set_tim(tim)
+
+
+class Tuner:
+    def __init__(self, cache_path=None, steps: int = 6, reps: int = 2, use_cache: bool = True):
+        self.cache_path = Path(cache_path) if cache_path else default_cache_path()
+        self.steps = steps
+        self.reps = reps
+        self.use_cache = use_cache
+        self.log = []  # (what, choice, seconds) of every timing taken
+
+    # ------------------------------------------------------------ cache
+    def _load(self) -> dict:
+        try:
+            return json.loads(self.cache_path.read_text())
+        except (OSError, ValueError):
+            return {}
+
+    def _store(self, key: str, value) -> None:
+        data = self._load()
+        data[key] = value
+        try:
+            self.cache_path.parent.mkdir(parents=True, exist_ok=True)
+            tmp = self.cache_path.with_suffix(".tmp")
+            tmp.write_text(json.dumps(data, indent=1, sort_keys=True))
+            tmp.replace(self.cache_path)
+        except OSError:
+            pass  # a read-only home is not an error: the choice still applies
+
+    # ---------------------------------------------------------- timing
+    def _best(self, options, apply, run):
+        """Apply each option, time run(), keep the fastest (min over reps)."""
+        best, best_t = None, float("inf")
+        for opt in options:
+            try:
+                apply(opt)
+            except PipeflowError:  # a tile over the shared-memory cap
+                continue
+            t = min(run() for _ in range(self.reps))
+            self.log.append((opt, t))
+            if t < best_t:
+                best, best_t = opt, t
+        apply(best)
+        return best, best_t
+
+    # ------------------------------------------------------------ a pipe
+    def tune_pipe(self, pipe) -> dict:
+        """Choose the launch choices of one pipe by timing it alone."""
+        key = "pipe:" + _shape_key(shape_of(pipe))
+        if self.use_cache:
+            hit = self._load().get(key)
+            if hit:
+                pipe.set_tuning(**hit)
+                return hit
+        snap = _Snapshot([pipe])
+        cur = {"ld_solver": L.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 0}
+
+        def run():
+            pipe.steporbit(2)
+            pipe.sync()
+            t0 = time.perf_counter()
+            pipe.steporbit(self.steps)
+            pipe.sync()
+            return time.perf_counter() - t0
+
+        for knob, values in (("ld_solver", (L.PF_LD_AUTO, L.PF_LD_REBUILT)),
+                             ("nl_mc", _mc_candidates(pipe.M)), ("nl_zc", ZC_CANDIDATES)):
+            def apply(v, knob=knob):
+                pipe.set_tuning(**dict(cur, **{knob: v}))
+                cur[knob] = v
+            self._best(values, apply, run)
+        snap.restore()
+        self._store(key, dict(cur))
+        return dict(cur)
+
+    # ----------------------------------------------------------- a batch
+    def tune_batch(self, batch) -> dict:
+        """Choose the launch choices of every pipe shape of a batch by timing
+        whole batch steps; returns {shape key: choice}."""
+        shapes = {}
+        for p in batch.pipes:
+            shapes.setdefault(shape_of(p), []).append(p)
+        sig = "batch:" + ",".join(f"{_shape_key(s)}x{len(v)}" for s, v in sorted(shapes.items()))
+        if self.use_cache:
+            hit = self._load().get(sig)
+            if hit and set(hit) == {_shape_key(s) for s in shapes}:
+                for s, pipes in shapes.items():
+                    for p in pipes:
+                        p.set_tuning(**hit[_shape_key(s)])
+                return hit
+        snap = _Snapshot(batch.pipes)
+        choice = {s: {"ld_solver": L.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 0} for s in shapes}
+
+        def run():
+            batch.step(3, orbit=True)  # rebuild after a change: direct step, capture, replay
+            batch.sync()
+            t0 = time.perf_counter()
+            batch.step(self.steps, orbit=True)
+            batch.sync()
+            return time.perf_counter() - t0
+
+        # largest shapes first: they carry most of the step
+        order = sorted(shapes, key=lambda s: -s[0] * s[1] * s[2] * len(shapes[s]))
+        for knob in ("ld_solver", "nl_mc", "nl_zc"):
+            for s in order:
+                values = {"ld_solver": (L.PF_LD_AUTO, L.PF_LD_REBUILT), "nl_mc": _mc_candidates(s[2]),
+                          "nl_zc": ZC_CANDIDATES}[knob]
+
+                def apply(v, s=s, knob=knob):
+                    new = dict(choice[s], **{knob: v})
+                    for p in shapes[s]:
+                        p.set_tuning(**new)
+                    choice[s] = new
+                self._best(values, apply, run)
+        snap.restore()
+        out = {_shape_key(s): c for s, c in choice.items()}
+        self._store(sig, out)
+        return out

@@ -1,0 +1,138 @@
+"""Launch choices (pf_ctx_set_tuning) change the speed, never the numbers.
+
+The Helmholtz solves of the fused step either stream the banded LU factors
+that k_lu_factor stored (PF_LD_STREAMED, the built-in choice) or rebuild them
+on chip in the same order of operations (PF_LD_REBUILT, for factorisations
+that did not pivot);
+the transform passes take any z-pass column tile and any even theta-pass row
+tile.  Each pair of pipes here starts from the same seeded state and must
+stay bitwise equal step after step, and one of them is held to the oracle.
+"""
+import numpy as np
+import pytest
+
+import pipeflow_oracle as O
+from _util import CFG1, SMALL, device_pipe, oracle_pipe, state_from_dev, state_to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+def _states_equal(a, b):
+    for (ar, ai), (br, bi) in zip(a.get_state(), b.get_state()):
+        if not (np.array_equal(ar, br) and np.array_equal(ai, bi)):
+            return False
+    return True
+
+
+def _pair(cfgd, **extra):
+    a, b = device_pipe(cfgd, **extra), device_pipe(cfgd, **extra)
+    for g in (a, b):
+        g.vel_matrices()
+    return a, b
+
+
+@pytest.mark.parametrize("cfgd", [SMALL[0], SMALL[1], CFG1], ids=["small0", "small1", "cfg1"])
+@pytest.mark.parametrize("mixed", [False, True], ids=["fp64", "mixed"])
+def test_helmholtz_factors_rebuilt_on_chip_equal_streamed(cfgd, mixed):
+    import pipeflow as P
+    extra = {"precision": P.PF_PREC_MIXED} if mixed else {}
+    a, b = _pair(cfgd, **extra)
+    a.set_tuning(ld_solver=P.PF_LD_REBUILT)
+    b.set_tuning(ld_solver=P.PF_LD_STREAMED)
+    assert a.get_tuning()["ld_solver"] == P.PF_LD_REBUILT
+    o = oracle_pipe(cfgd)
+    o.vel_matrices()
+    st = O.seeded_state(o, 3, 1e-3)
+    for g in (a, b):
+        state_to_dev(g, st)
+    for _ in range(4):
+        assert a.timestep() == b.timestep()
+        assert _states_equal(a, b)
+    a.steporbit(2)
+    b.steporbit(2)
+    assert _states_equal(a, b)
+    if not mixed:
+        o.set_state(*st)
+        for _ in range(4):
+            o.timestep()
+        for _ in range(2):
+            o.timestep(orbit=True)
+        assert O.rel_l2(state_from_dev(a), o.state()) <= 1e-12
+
+
+@pytest.mark.parametrize("mixed", [False, True], ids=["fp64", "mixed"])
+def test_transform_tiles_do_not_change_results(mixed):
+    import pipeflow as P
+    extra = {"precision": P.PF_PREC_MIXED} if mixed else {}
+    ref = device_pipe(CFG1, **extra)
+    ref.vel_matrices()
+    P.seeded_state(ref, 11, 1e-3)
+    start = ref.get_state()
+    for _ in range(2):
+        ref.timestep()
+    for mc, zc in [(1, 2), (3, 4), (16, 8), (5, 16), (0, 6)]:
+        g = device_pipe(CFG1, **extra)
+        g.vel_matrices()
+        g.set_tuning(nl_mc=mc, nl_zc=zc)
+        g.set_state(*start)
+        for _ in range(2):
+            g.timestep()
+        assert _states_equal(g, ref), (mc, zc)
+        g.close()
+    ref.close()
+
+
+def test_tuning_rejects_bad_choices():
+    import pipeflow as P
+    g = device_pipe(SMALL[0])
+    with pytest.raises(Exception):
+        g.set_tuning(nl_zc=3)
+    with pytest.raises(Exception):
+        g.set_tuning(ld_solver=7)
+    g.set_tuning(ld_solver=P.PF_LD_REBUILT)
+    g.set_tuning()
+    assert g.get_tuning() == {"ld_solver": P.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 0}
+
+
+def _batch(cfgs):
+    import pipeflow as P
+    b = P.Batch([P.PipeConfig(**d) for d in cfgs])
+    b.matrices()
+    for i, p in enumerate(b.pipes):
+        P.seeded_state(p, 40 + i, 1e-3)
+    return b
+
+
+def test_autotuned_batch_equals_untuned(tmp_path):
+    """The tuner restores the states it advanced while timing, caches its
+    choices, and a tuned batch steps bit for bit like an untuned one."""
+    import pipeflow as P
+    mix = [dict(SMALL[0]), dict(SMALL[1]), dict(SMALL[0], precision=P.PF_PREC_MIXED),
+           dict(CFG1, precision=P.PF_PREC_MIXED)]
+    a, b = _batch(mix), _batch(mix)
+    tuner = P.Tuner(cache_path=tmp_path / "tuning.json", steps=2, reps=1)
+    choice = tuner.tune_batch(a)
+    assert len(choice) == 4 and len(tuner.log) > 8
+    for pa, pb in zip(a.pipes, b.pipes):
+        assert _states_equal(pa, pb)
+        assert pa.tim.step == pb.tim.step
+    a.step(3)
+    b.step(3)
+    for pa, pb in zip(a.pipes, b.pipes):
+        assert _states_equal(pa, pb)
+    again = P.Tuner(cache_path=tmp_path / "tuning.json", steps=2, reps=1)
+    assert again.tune_batch(a) == choice and again.log == []
+
+
+def test_autotuned_pipe_equals_untuned(tmp_path):
+    import pipeflow as P
+    a, b = _pair(CFG1)
+    P.seeded_state(a, 12, 1e-3)
+    b.set_state(*a.get_state())
+    t = P.Tuner(cache_path=tmp_path / "tuning.json", steps=2, reps=1)
+    t.tune_pipe(a)
+    assert _states_equal(a, b)
+    for _ in range(3):
+        a.timestep()
+        b.timestep()
+    assert _states_equal(a, b)

@@ -1,5 +1,5 @@
 """util plug-ins through main.f90's var_null hook (Coriolis.f90,
-nonnewtonian.f90) and the host callback.
+nonnewtonian.f90, LES.f90) and the host callback.
 
 CPU: invariants of the oracle's restatements.  GPU: pf_timestep with each
 built-in plug-in against the oracle's main loop with the same plug-in, the
@@ -48,8 +48,13 @@ def test_carreau_yasuda_newtonian_limit_adds_nothing():
     assert O.rel_l2([o.vel_Nr, o.vel_Nt, o.vel_Nz], N0) < 1e-10
 
 
+SMAG = (1.0, 0.025, 1.0, 25.0)   # model, C_s, filter, A_plus (LES.f90:4-6)
+VREMAN = (2.0, 0.03, 2.0, 0.0)   # (LES.f90:8-10)
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", ["coriolis", "carreau_yasuda"])
+@pytest.mark.parametrize("kind", ["coriolis", "carreau_yasuda", "les_smagorinsky", "les_vreman",
+                                  "les_smagorinsky_filter3", "les_vreman_filter3"])
 def test_plugin_steps_match_oracle(kind):
     import pipeflow as P
     o, st = _oracle(CFG)
@@ -59,17 +64,32 @@ def test_plugin_steps_match_oracle(kind):
     if kind == "coriolis":
         g.util_set(P._lib.PF_UTIL_CORIOLIS, (0.5, 0.3))
         util = lambda op: UO.coriolis(op, 0.5, 0.3)  # noqa: E731
-    else:
+    elif kind == "carreau_yasuda":
         g.util_set(P._lib.PF_UTIL_CARREAU_YASUDA, CY)
         o.tim_pcn = 1  # nonnewtonian.f90:66-67
         o.tim_it = 0
         stats = []
         util = lambda op: stats.append(UO.carreau_yasuda(op, *CY))  # noqa: E731
+    else:
+        par = list(SMAG if "smagorinsky" in kind else VREMAN)
+        if kind.endswith("filter3"):
+            par[2] = 3.0
+            par[3] = 25.0
+        g.util_set(P._lib.PF_UTIL_LES, par)
+        util = UO.LES(o, *par)
     for _ in range(3):
         no = UO.timestep_with_util(o, util)
         ng = g.timestep()
         assert no == ng
     assert O.rel_l2(state_from_dev(g), o.state()) <= 1e-11
+    if kind.startswith("les"):
+        # update_nu_r moved the reference viscosity (and the matrices) alike
+        assert g.vel_nu == pytest.approx(o.vel_nu, rel=1e-12)
+        if "smagorinsky" in kind:
+            assert o.vel_nu > 1.0
+        wall, lo, hi = g.util_nu_stats()
+        assert hi == pytest.approx(util.nu_max, rel=1e-11)
+        assert hi > 0.0 and lo >= 0.0
     if kind == "carreau_yasuda":
         wall, lo, hi = g.util_nu_stats()
         assert wall == pytest.approx(stats[-1][0], rel=1e-11)
@@ -166,3 +186,51 @@ def test_coriolis_on_laminar_flow_is_the_analytic_force():
     for got, base, want in ((o.vel_Nr, N0[0], want_r), (o.vel_Nt, N0[1], want_t), (o.vel_Nz, N0[2], z)):
         assert np.max(np.abs(got.re - base.re - want.re)) < tol
         assert np.max(np.abs(got.im - base.im - want.im)) < tol
+
+
+def test_les_vreman_vanishes_on_laminar_flow():
+    """Vreman's invariant P of B = Delta^2 A^T A is zero for a gradient of rank
+    one, so for Hagen-Poiseuille flow alone (only dU/dr) nu_t = 0 and, with the
+    reference viscosity at 1, the plug-in adds nothing."""
+    o = oracle_pipe(dict(N=40, K=3, M=3, Mp=1, Re=2000.0, alpha=1.25, dt=0.01))
+    o.vel_matrices()
+    z = O.Coll.zeros(o.N, o.H)
+    o.vel_Nr, o.vel_Nt, o.vel_Nz = z.copy(), z.copy(), z.copy()
+    o.vel_ur, o.vel_ut, o.vel_uz = z.copy(), z.copy(), z.copy()
+    les = UO.LES(o, *VREMAN)
+    u, S = les.get_nu(o)
+    assert np.max(np.abs(les.nu)) == 0.0
+    les.update_nonlin_terms(o, u, S)
+    assert max(np.max(np.abs(c.re)) + np.max(np.abs(c.im)) for c in (o.vel_Nr, o.vel_Nt, o.vel_Nz)) < 1e-12
+
+
+def test_les_smagorinsky_on_laminar_flow_matches_the_model():
+    """For Hagen-Poiseuille flow alone: the strain rate is |U'| = 2r, u_tau =
+    sqrt(2/Re) (the wall derivative of U), so nu_t(r) = vanDr (C_s Delta)^2 2r
+    with the van Driest factor 1 - exp(-(Re u_tau (1-r) / A+)^2); the added
+    term is axisymmetric and axial only: in the mean mode
+    N'_z = (1/Re)(Re nu_t + 1 - nu_r)(-4) - 4 nu_t - 2 r d(nu_t)/dr,
+    (curl curl U = 4 z, 2 grad(nu_t).S has S_rz = U'/2 = -r), with the radial
+    derivative that of the 9-point finite differences."""
+    o = oracle_pipe(dict(N=40, K=3, M=3, Mp=1, Re=2000.0, alpha=1.25, dt=0.01))
+    o.vel_matrices()
+    z = O.Coll.zeros(o.N, o.H)
+    o.vel_Nr, o.vel_Nt, o.vel_Nz = z.copy(), z.copy(), z.copy()
+    o.vel_ur, o.vel_ut, o.vel_uz = z.copy(), z.copy(), z.copy()
+    les = UO.LES(o, *SMAG)
+    u, S = les.get_nu(o)
+    r = o.mes_D.r
+    Re = o.cfg.Re
+    assert les.u_tau == pytest.approx(np.sqrt(2.0 / Re), rel=1e-12)
+    Delta = (les.Delta_r * les.Rdth * les.dz) ** (1.0 / 3.0)
+    vanDr = 1.0 - np.exp(-(Re * np.sqrt(2.0 / Re) * (1.0 - r) / SMAG[3]) ** 2)
+    nut = vanDr * (SMAG[1] * Delta) ** 2 * 2.0 * r
+    assert np.max(np.abs(les.nu - nut[:, None, None])) < 1e-12 * np.max(nut)
+    les.update_nonlin_terms(o, u, S)
+    dnut = o.var_coll_meshmult(o.mes_D.dr[0], O.Coll(nut[:, None] * np.ones((1, o.H)), np.zeros((o.N, o.H)))).re[:, 0]
+    want = (1.0 / Re) * (Re * nut + 1.0 - o.vel_nu) * (-4.0) - 4.0 * nut - 2.0 * r * dnut
+    got = o.vel_Nz.re[:, 0]
+    scale = np.max(np.abs(want))
+    assert np.max(np.abs(got - want)) < 1e-10 * scale
+    assert np.max(np.abs(o.vel_Nr.re)) + np.max(np.abs(o.vel_Nt.re)) < 1e-10 * scale
+    assert np.max(np.abs(o.vel_Nz.re[:, 1:])) + np.max(np.abs(o.vel_Nz.im)) < 1e-10 * scale
