@@ -61,6 +61,16 @@ def batched_configs(npipes: int = 64, seed: int = 3):
     return out
 
 
+def transform_flops(d):
+    """FFT flops of one nonlinear evaluation of a pipe (5 L log2 L per complex
+    FFT of length L): six inverse and three forward z transforms of length 3K
+    over M columns, and per z-row pair six inverse and three forward packed
+    theta transforms of length 3M, at each radial point."""
+    Z, Th = 3 * d["K"], 3 * d["M"]
+    fz, ft = 5 * Z * math.log2(Z), 5 * Th * math.log2(Th)
+    return d["N"] * (9 * d["M"] * fz + 9 * (Z / 2) * ft)
+
+
 def harmonics_count(d):
     return (2 * d["K"] - 1) * d["M"] - (d["K"] - 1)
 
@@ -381,7 +391,7 @@ def run_batched(args, torch, P, dist, world, rank, local):
     master = torch.cuda.ExternalStream(h.value)
     tuned = None
     if args.ld_solver != "auto":  # one Helmholtz solver for every pipe (profiling)
-        ld = {"streamed": P.PF_LD_STREAMED, "rebuilt": P.PF_LD_REBUILT}[args.ld_solver]
+        ld = {"streamed": P.PF_LD_STREAMED, "rebuilt": P.PF_LD_REBUILT, "paired": P.PF_LD_PAIRED}[args.ld_solver]
         for p in batch.pipes:
             p.set_tuning(ld_solver=ld)
     if args.tune:
@@ -394,11 +404,18 @@ def run_batched(args, torch, P, dist, world, rank, local):
     batch.step(args.spinup if args.spinup is not None else 20)
     batch.prof_enable(True)
     batch.step(args.warmup)
-    # the dominant category among the stage-batched launches, whose every
-    # span covers all pipes (a pipe's own extra corrector pass is left out)
+    # the dominant kernel among the stage-batched launches, whose every span
+    # covers all pipes (a pipe's own extra corrector pass is left out): the
+    # categories timed as one kernel's launches (the transform categories
+    # each span several launches, one per transform length, run side by
+    # side; they are reported together as the transform chain below)
     staged0 = batch.staged()
     prof = batch.prof_read(staged_only=staged0)
-    dom = max(prof, key=lambda k: prof[k][0])
+    single = ("lusolve", "ppe", "infl")
+    dom = max(single, key=lambda k: prof[k][0])
+    nl_evals = max(prof["thfwd"][1], 1)
+    chain_ms = (prof["zinv"][0] + prof["thfwd"][0] + prof["zfwd"][0]) / nl_evals
+    chain_share = (prof["zinv"][0] + prof["thfwd"][0] + prof["zfwd"][0]) / max(sum(v[0] for v in prof.values()), 1e-30)
     batch.prof_enable([dom])
     batch.step(2)  # re-capture both parities with the dominant category's event nodes
     batch.prof_enable([dom])
@@ -457,8 +474,20 @@ def run_batched(args, torch, P, dist, world, rank, local):
     # covers every pipe, a per-pipe launch one pipe (averaged over the pipes)
     per_launch = PER_LAUNCH_S[dom] * (sum(S) if staged else sum(S) / len(S))
     io = sum(6 * d["N"] * harmonics_count(d) * 8 for d in cfgs)
+    chain_bytes = 6 * sum(S)   # u in, N out
+    chain_flops = sum(transform_flops(d) for d in cfgs)
     extra = {"corrector_iterations_per_step": nc, "algorithmic_bytes_per_batch_step": step_bytes,
              "stage_batched": staged, "autotune": tuned,
+             "transform_roofline": {
+                 "scope": "one evaluation of the nonlinear terms of every pipe: FP64 mean-mode pass (and curl), "
+                          "z inverse, theta pass with u x curl(u), z forward (all transform launches)",
+                 "avg_evaluation_us": chain_ms * 1e3, "share_of_step_kernels": chain_share,
+                 "algorithmic_bytes": chain_bytes, "achieved_gbs": chain_bytes / (chain_ms / 1e3) / 1e9,
+                 "frac_of_measured_hbm": chain_bytes / (chain_ms / 1e3) / 1e9 / peaks()[0],
+                 "fft_flops": chain_flops, "achieved_fp32_tflops": chain_flops / (chain_ms / 1e3) / 1e12,
+                 "fp32_nominal_tflops": 74.4,
+                 "note": "flops by the 5 L log2 L count per complex FFT of length L; the FP32 peak is the nominal "
+                         "148 SMs x 128 lanes x 2 x 1.965 GHz (not measured)"},
              "batch_step_ms": ms / args.steps,
              "step_roofline": {"bound": "hbm", "scope": "whole batch step (all stages, all pipes)",
                                "achieved": step_bytes / (ms / args.steps / 1e3) / 1e9, "unit": "GB/s"}}
@@ -470,6 +499,7 @@ def run_batched(args, torch, P, dist, world, rank, local):
         extra["batched_over_plain"] = (args.pipes * args.steps / (ms / 1e3)) / plain
         extra["mixed_vs_fp64"] = mixed_error(P, {k: SINGLE["cfg1"][k] for k in PHYS}, SINGLE["cfg1"]["seed"],
                                              args.err_steps, SINGLE["cfg1"]["energy"])
+        extra["util_plugins"] = util_plugin_timing(P, torch, local)
         if args.with_serve:
             extra["serve"] = run_serve(args, P, local, plain)
         if args.with_cfg2 and not args.no_cpu_baseline:
@@ -501,6 +531,37 @@ def run_batched(args, torch, P, dist, world, rank, local):
 
 
 KRYLOV = dict(N=48, K=32, M=24, Mp=1, Re=2000.0, alpha=1.25)
+
+
+def util_plugin_timing(P, torch, local, steps=100):
+    """ms per main-loop step of the config-1 pipe (FP64) with each built-in
+    plug-in of main.f90's var_null hook: Coriolis and Carreau-Yasuda run
+    inside the step graphs, LES eagerly (its update_nu_r reads max nu_t back
+    to the host)."""
+    from pipeflow import _lib as L
+    kinds = {"none": None, "coriolis": (L.PF_UTIL_CORIOLIS, (0.5, 0.3)),
+             "carreau_yasuda": (L.PF_UTIL_CARREAU_YASUDA, (1000.0, 0.01, 0.05, 0.0035, 3.3, 0.36, 2.0)),
+             "les_smagorinsky": (L.PF_UTIL_LES, (1.0, 0.025, 1.0, 25.0))}
+    out = {}
+    stream = torch.cuda.Stream()
+    for name, k in kinds.items():
+        p = P.Pipe(P.PipeConfig(**{q: SINGLE["cfg1"][q] for q in PHYS}), device=local)
+        p.lib.pf_ctx_set_stream(p.ctx, stream.cuda_stream)
+        p.vel_matrices()
+        P.seeded_state(p, 1, 1e-3)
+        if k:
+            p.util_set(*k)
+        for _ in range(3):
+            p.timestep()
+        e0, e1 = dev_timer(torch, stream)
+        e0.record(stream)
+        for _ in range(steps):
+            p.timestep()
+        e1.record(stream)
+        stream.synchronize()
+        out[name] = e0.elapsed_time(e1) / steps
+        p.close()
+    return {"ms_per_step": out, "what": "N=40 K=24 M=16 FP64 pf_timestep, 100 steps"}
 
 
 def run_serve(args, P, local, plain_value):
@@ -585,7 +646,7 @@ def main():
     ap.add_argument("--sustained-rates", type=float, nargs="+", default=[2.0, 4.0, 8.0, 16.0])
     ap.add_argument("--sustained-window", type=float, default=2.0)
     ap.add_argument("--no-tune", dest="tune", action="store_false")
-    ap.add_argument("--ld-solver", default="auto", choices=["auto", "streamed", "rebuilt"])
+    ap.add_argument("--ld-solver", default="auto", choices=["auto", "streamed", "rebuilt", "paired"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 

@@ -105,6 +105,8 @@ int pf_ctx_set_stream(pf_ctx *ctx, void *cuda_stream);
 #define PF_LD_STREAMED 1  /* Helmholtz factors streamed from HBM */
 #define PF_LD_REBUILT  2  /* Helmholtz factors rebuilt on chip (factorisations
                              that did not pivot, N >= 10; else streamed) */
+#define PF_LD_PAIRED   3  /* streamed factors, modes k and -k paired on one
+                             factor stream (pressure and Helmholtz solves) */
 typedef struct {
     int ld_solver; /* PF_LD_* */
     int nl_mc;     /* z-pass columns per block (1..M; 0 = built-in) */

@@ -303,7 +303,8 @@ extern "C" int pf_ctx_set_stream(pf_ctx *ctx, void *stream) {
 
 extern "C" int pf_ctx_set_tuning(pf_ctx *ctx, const pf_tuning *t) {
     PF_ARG(ctx && t, "pf_ctx_set_tuning: null argument");
-    PF_ARG(t->ld_solver == PF_LD_AUTO || t->ld_solver == PF_LD_STREAMED || t->ld_solver == PF_LD_REBUILT,
+    PF_ARG(t->ld_solver == PF_LD_AUTO || t->ld_solver == PF_LD_STREAMED || t->ld_solver == PF_LD_REBUILT ||
+               t->ld_solver == PF_LD_PAIRED,
            "pf_ctx_set_tuning: bad ld_solver");
     PF_TRY(pf_nl_tiles_check(ctx, t));
     if (std::memcmp(&ctx->tune, t, sizeof(pf_tuning)) == 0) return PF_OK;

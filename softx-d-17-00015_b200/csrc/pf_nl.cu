@@ -93,15 +93,18 @@ __device__ __forceinline__ void nl_zinv_body(const NLArgs &a, int bx, int by, in
     const int comp = bz, n = by, m0 = bx * MC;
     const int mc = min(MC, g.M - m0);
     fft4_tables<ZL>(tw, tw2, twz);
-    // curl(u) of the mixed-precision path was formed once by the mean-mode
-    // pass; else each input is formed here (u, or curl(u) from 9-row stencils)
+    // FP32 transforms (mixed precision): u, or the curl(u) the mean-mode pass
+    // formed once; FP64: u, or curl(u) from 9-row stencils here
     const float2 *__restrict__ cf = (a.curlf && comp >= 3) ? a.curlf + (size_t)((comp - 3) * g.N + n) * g.Hp : nullptr;
+    const double2 *__restrict__ uc = comp < 3 ? pick3(a.u, comp) + (size_t)n * g.Hp : nullptr;
     auto input = [&](int nh, int k, int m) -> C {
         if constexpr (sizeof(C) == 8) {
-            if (cf) return cf[nh];
+            return comp >= 3 ? cf[nh] : to_c<C>(uc[nh]);
+        } else {
+            return to_c<C>(nl_input(a, comp, n, nh, k, m));
         }
-        return to_c<C>(nl_input(a, comp, n, nh, k, m));
     };
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < mc * ZL; idx += blockDim.x) {
         const int c = idx / ZL, j = idx - c * ZL;
         const int m = m0 + c;
@@ -145,8 +148,8 @@ __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
     const int M = g.M, Z = g.Z, np = ZC / 2;
     const int rowsA = 3 * ZC;  // six components x ZC/2 packed pairs
     C *bufA = reinterpret_cast<C *>(smraw);
-    C *bufB = bufA + (FR::smem_elems(rowsA) - 2 * TL);
-    C *tw = bufB + (FR::smem_elems(rowsA / 2) - 2 * TL), *tw2 = tw + TL;
+    // the products overwrite the first three components' rows in place
+    C *tw = bufA + (FR::smem_elems(rowsA) - 2 * TL), *tw2 = tw + TL;
     const int n = by, z0 = bx * ZC;
     fft4_tables<TL>(tw, tw2, twt);
     for (int i = threadIdx.x; i < rowsA * RS; i += blockDim.x) bufA[i] = CTraits<C>::make(0, 0);
@@ -154,6 +157,7 @@ __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
     // Hermitian-extend the M retained theta modes of two z rows into one
     // complex row: X = a + i b (c2r ignores the DC imaginary parts)
     const float inp = 1.0f / np, inM = 1.0f / M;
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < 6 * M * np; idx += blockDim.x) {
         const int rest = fdiv(idx, np, inp), zp = idx - rest * np;
         const int comp = fdiv(rest, M, inM), m = rest - comp * M;
@@ -172,7 +176,7 @@ __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
     __syncthreads();
     FR::template run<+1>(bufA, rowsA, tw, tw2);
     const C *phys = bufA;
-    C *prod = bufB;
+    C *prod = bufA;  // row (c*np + zp) of component c < 3: read above, then rewritten by the same thread
     // u x curl(u) (velocity.f90:325-329), scaled for the forward transform
     const R base = (R)(1.0 - a.dm.rp[4 * g.N + n] * a.dm.rp[4 * g.N + n]);
     R mr = 0, mt = 0, mz = 0;
@@ -255,30 +259,34 @@ __device__ __forceinline__ void nl_zfwd_body(const NLArgs &a, int bx, int by, in
     FR::template run<-1>(rows, mc, tw, tw2);
     const C *res = rows;
     const double U = a.dm.velU[n], b = -a.dm.velUp[n];
+    // the constant-flux pressure Pr0 enters at k = m = 0 only: the first
+    // m-chunk of the axial component needs it (vel_addHPF, velocity.f90:355-359)
     double Pr0 = 0.0;
-    if (comp == 2 && a.const_flux) {
+    if (comp == 2 && a.const_flux && m0 == 0) {
         for (int j = 0; j <= KL; ++j) Pr0 += a.u[2][(size_t)(g.N - 1 - KL + j) * g.Hp].x * a.dm.dr1[1 * (KL + 1) + j];
         Pr0 = Pr0 / (-2.0);
-        if (n == 0 && m0 == 0 && threadIdx.x == 0) a.sc->Pr0 = Pr0;
+        if (n == 0 && threadIdx.x == 0) a.sc->Pr0 = Pr0;
     }
-    double2 *f = pick3(a.N, comp) + (size_t)n * g.Hp;
+    double2 *__restrict__ f = pick3(a.N, comp) + (size_t)n * g.Hp;
+    const double2 *__restrict__ uc = pick3(a.u, comp) + (size_t)n * g.Hp;
+    const double2 *__restrict__ ur0 = a.u[0] + (size_t)n * g.Hp;
     const float ik = 1.0f / (2 * K - 1);
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < mc * (2 * K - 1); idx += blockDim.x) {
         const int c = fdiv(idx, 2 * K - 1, ik), kk = idx - c * (2 * K - 1) - (K - 1);
         const int m = m0 + c;
         if (m == 0 && kk < 0) continue;
         const int nh = m * (2 * K - 1) + kk;
         const C x = res[c * RS + (kk >= 0 ? kk : ZL + kk)];
-        const size_t at = (size_t)n * g.Hp + nh;
         const double av = g.alpha * kk * U;
         double2 o = make_double2((double)x.x, (double)x.y);
+        const double2 v = uc[nh];
         if (comp == 2) {
-            const double2 vz = a.u[2][at], vr = a.u[0][at];
-            o.x = o.x + av * vz.y + b * vr.x;
-            o.y = o.y - av * vz.x + b * vr.y;
+            const double2 vr = ur0[nh];
+            o.x = o.x + av * v.y + b * vr.x;
+            o.y = o.y - av * v.x + b * vr.y;
             if (nh == 0 && a.const_flux) o.x = o.x + 4.0 * Pr0 / g.Re;
         } else {
-            const double2 v = pick3(a.u, comp)[at];
             o.x = o.x + av * v.y;
             o.y = o.y - av * v.x;
         }
@@ -350,9 +358,7 @@ template <typename C> struct NLTiles {
 };
 static constexpr size_t NL_TILE_MAX_SMEM = 100 * 1024;  // largest tile a tuning may choose
 
-template <typename C> static size_t theta_smem(int Th, int ZC) {
-    return (size_t)(rows_elems<C>(Th, 3 * ZC) + rows_elems<C>(Th, 3 * ZC / 2)) * sizeof(C);
-}
+template <typename C> static size_t theta_smem(int Th, int ZC) { return (size_t)rows_elems<C>(Th, 3 * ZC) * sizeof(C); }
 
 // Tiles of the three transform passes: the tuning's choice where it set one,
 // else the built-in rule.

@@ -340,6 +340,242 @@ __device__ __forceinline__ void solve_async(const double *__restrict__ lu, const
 #undef RSLOT
 }
 
+// The same banded solve for two right-hand sides through one factor
+// stream: modes (k, m) and (-k, m) have the same matrix (bitwise, see
+// lumesh_entry) and therefore the same factors and pivots, so one thread
+// solves the real (or imaginary) parts of both and every factor value is
+// fetched once for the two.  rhsB/outB belong to the mirror mode; with
+// twin false the second chain is idle.  Each chain's operations are those of
+// solve_async, so the solutions are bitwise the same.
+template <bool PIV, int TS>
+__device__ __forceinline__ void solve_async2(const double *__restrict__ lu, const double *__restrict__ pivd, int N,
+                                             int Hp, int nh, const double *__restrict__ rhsA,
+                                             const double *__restrict__ rhsB, size_t rs, double *outA, double *outB,
+                                             size_t os, bool twin, double *ring) {
+    constexpr int KU = PIV ? KV : KL;
+    constexpr int SWF = KL + 2 + (PIV ? 1 : 0);  // forward slot: L column, two rhs ahead, pivot
+    constexpr int SWB = KU + 1;                  // backward slot: U column
+    constexpr int SW = SWF > SWB ? SWF : SWB;
+    constexpr unsigned QB = 8u * TS, SB = 8u * TS * SW;
+    const size_t rowst = (size_t)N * Hp;
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(ring);
+#define RSLOT(s, q) ring[((s) * SW + (q)) * TS]
+    const double *Lj = lu + (size_t)(KV + 1) * rowst + nh;
+    const double *Pj = PIV ? pivd + nh : nullptr;
+    const double *RAj = rhsA + (size_t)(KL + 1) * rs;
+    const double *RBj = rhsB + (size_t)(KL + 1) * rs;
+    int jj = 0;
+    auto issue_fwd = [&](int s) {
+        if (jj < N) {
+            if (jj < N - 1) {
+#pragma unroll
+                for (int i = 0; i < KL; ++i) cp_async8s(sbase + s * SB + i * QB, Lj + i * rowst);
+                if (PIV) cp_async8s(sbase + s * SB + (KL + 2) * QB, Pj);
+            }
+            if (jj + KL + 1 < N) {
+                cp_async8s(sbase + s * SB + KL * QB, RAj);
+                if (twin) cp_async8s(sbase + s * SB + (KL + 1) * QB, RBj);
+            }
+        }
+        cp_async_commit();
+        ++jj;
+        Lj += Hp;
+        if (PIV) Pj += Hp;
+        RAj += rs;
+        RBj += rs;
+    };
+    double wa[KL + 1], wb[KL + 1];
+#pragma unroll
+    for (int i = 0; i <= KL; ++i) {
+        wa[i] = (i < N) ? rhsA[(size_t)i * rs] : 0.0;
+        wb[i] = (i < N && twin) ? rhsB[(size_t)i * rs] : 0.0;
+    }
+#pragma unroll
+    for (int s = 0; s < RING; ++s) issue_fwd(s);
+    double *OAj = outA, *OBj = outB;
+    for (int j0 = 0; j0 < N; j0 += RING) {
+#pragma unroll
+        for (int s = 0; s < RING; ++s) {
+            const int j = j0 + s;
+            if (j < N) {
+                cp_async_wait<RING - 1>();
+                const double aheadA = (j + KL + 1 < N) ? RSLOT(s, KL) : 0.0;
+                const double aheadB = (j + KL + 1 < N && twin) ? RSLOT(s, KL + 1) : 0.0;
+                if (j < N - 1) {
+                    if (PIV) {
+                        const int p = (int)RSLOT(s, KL + 2);
+#pragma unroll
+                        for (int i = 1; i <= KL; ++i)
+                            if (p == i) {
+                                const double t = wa[0];
+                                wa[0] = wa[i];
+                                wa[i] = t;
+                                const double u = wb[0];
+                                wb[0] = wb[i];
+                                wb[i] = u;
+                            }
+                    }
+                    const double bja = wa[0], bjb = wb[0];
+#pragma unroll
+                    for (int i = 1; i <= KL; ++i)
+                        if (j + i < N) {
+                            const double L = RSLOT(s, i - 1);
+                            wa[i] = fma(-L, bja, wa[i]);
+                            wb[i] = fma(-L, bjb, wb[i]);
+                        }
+                }
+                *OAj = wa[0];
+                if (twin) *OBj = wb[0];
+                OAj += os;
+                OBj += os;
+#pragma unroll
+                for (int i = 0; i < KL; ++i) {
+                    wa[i] = wa[i + 1];
+                    wb[i] = wb[i + 1];
+                }
+                wa[KL] = aheadA;
+                wb[KL] = aheadB;
+                issue_fwd(s);
+            }
+        }
+    }
+    cp_async_wait<0>();
+    // back substitution with the U columns shared by the two chains
+    const double *Uj = lu + (size_t)KV * rowst + (size_t)(N - 1) * Hp + nh;
+    int tt = 0;
+    auto issue_bwd = [&](int s) {
+        if (tt < N) {
+#pragma unroll
+            for (int i = 0; i <= KU; ++i) cp_async8s(sbase + s * SB + i * QB, Uj - i * rowst);
+        }
+        cp_async_commit();
+        ++tt;
+        Uj -= Hp;
+    };
+#pragma unroll
+    for (int s = 0; s < RING; ++s) issue_bwd(s);
+    double va[KU + 1], vb[KU + 1];
+#pragma unroll
+    for (int i = 0; i <= KU; ++i) {
+        va[i] = (N - 1 - i >= 0) ? __ldcs(outA + (size_t)(N - 1 - i) * os) : 0.0;
+        vb[i] = (N - 1 - i >= 0 && twin) ? __ldcs(outB + (size_t)(N - 1 - i) * os) : 0.0;
+    }
+    constexpr int QY = 4;
+    double ya[QY], yb[QY];
+#pragma unroll
+    for (int q = 0; q < QY; ++q) {
+        const int r = N - 1 - KU - 1 - q;
+        ya[q] = (r >= 0) ? __ldcs(outA + (size_t)r * os) : 0.0;
+        yb[q] = (r >= 0 && twin) ? __ldcs(outB + (size_t)r * os) : 0.0;
+    }
+    double *XAj = outA + (size_t)(N - 1) * os, *XBj = outB + (size_t)(N - 1) * os;
+    for (int t0 = 0; t0 < N; t0 += RING) {
+#pragma unroll
+        for (int s = 0; s < RING; ++s) {
+            const int t = t0 + s;
+            if (t < N) {
+                const int j = N - 1 - t;
+                cp_async_wait<RING - 1>();
+                const double aheadA = ya[0], aheadB = yb[0];
+#pragma unroll
+                for (int q = 0; q < QY - 1; ++q) {
+                    ya[q] = ya[q + 1];
+                    yb[q] = yb[q + 1];
+                }
+                {
+                    const int r = j - KU - 1 - QY;
+                    ya[QY - 1] = (r >= 0) ? __ldcs(outA + (size_t)r * os) : 0.0;
+                    yb[QY - 1] = (r >= 0 && twin) ? __ldcs(outB + (size_t)r * os) : 0.0;
+                }
+                double xa = va[0], xb = vb[0];
+                if (xa != 0.0) {
+                    xa = xa / RSLOT(s, 0);
+#pragma unroll
+                    for (int i = 1; i <= KU; ++i)
+                        if (j - i >= 0) va[i] = fma(-xa, RSLOT(s, i), va[i]);
+                }
+                if (xb != 0.0) {
+                    xb = xb / RSLOT(s, 0);
+#pragma unroll
+                    for (int i = 1; i <= KU; ++i)
+                        if (j - i >= 0) vb[i] = fma(-xb, RSLOT(s, i), vb[i]);
+                }
+                *XAj = xa;
+                if (twin) *XBj = xb;
+                XAj -= os;
+                XBj -= os;
+#pragma unroll
+                for (int i = 0; i < KU; ++i) {
+                    va[i] = va[i + 1];
+                    vb[i] = vb[i + 1];
+                }
+                va[KU] = (j - KU - 1 >= 0) ? aheadA : 0.0;
+                vb[KU] = (j - KU - 1 >= 0) ? aheadB : 0.0;
+                issue_bwd(s);
+            }
+        }
+    }
+    cp_async_wait<0>();
+#undef RSLOT
+}
+
+// items of the paired solves: item = m*K + k (k >= 0); the primary mode
+// (k, m) and, for m >= 1 and k >= 1, its mirror (-k, m)
+__device__ __forceinline__ bool pair_item(const Geo &g, int item, int &nh, int &nh2) {
+    if (item >= g.M * g.K) return false;
+    const int m = item / g.K, k = item - m * g.K;
+    const int base = m * (2 * g.K - 1);
+    nh = m == 0 ? k : base + k;
+    nh2 = (m > 0 && k > 0) ? base - k : -1;
+    return true;
+}
+__host__ __device__ inline int pair_tiles(const Geo &g) { return (g.M * g.K + 31) / 32; }
+
+// S2 with the mirror modes paired: warp = (re or im) of 32 items
+__device__ __forceinline__ void solve_pnp2_body(const StepArgs &a, int bx) {
+    extern __shared__ double ring2p[];
+    const Geo &g = a.g;
+    const int part = threadIdx.x >> 5;
+    int nh, nh2;
+    if (!pair_item(g, bx * 32 + (threadIdx.x & 31), nh, nh2)) return;
+    const size_t st = 2 * (size_t)g.Hp;
+    const bool twin = nh2 >= 0;
+    const int nhb = twin ? nh2 : nh;
+    double *outA = reinterpret_cast<double *>(a.p) + 2 * (size_t)nh + part;
+    double *outB = reinterpret_cast<double *>(a.p) + 2 * (size_t)nhb + part;
+    const double *rhsA = reinterpret_cast<const double *>(a.prhs) + 2 * (size_t)nh + part;
+    const double *rhsB = reinterpret_cast<const double *>(a.prhs) + 2 * (size_t)nhb + part;
+    if (nh == 0) {  // BC=1 at k=m=0: zero (timestep.f90:110-113); no mirror
+        for (int n = 0; n < g.N; ++n) outA[n * st] = 0.0;
+        return;
+    }
+    solve_async2<true, 64>(a.lnp, a.pivd, g.N, g.Hp, nh, rhsA, rhsB, st, outA, outB, st, twin, ring2p + threadIdx.x);
+}
+
+// S4 with the mirror modes paired: warp = one (system, re/im) of 32 items
+__device__ __forceinline__ void solve_ld2_body(const StepArgs &a, int bx) {
+    extern __shared__ double ring4p[];
+    const Geo &g = a.g;
+    const int w = threadIdx.x >> 5;
+    const int sys = w >> 1, part = w & 1;
+    int nh, nh2;
+    if (!pair_item(g, bx * 32 + (threadIdx.x & 31), nh, nh2)) return;
+    const size_t st = 2 * (size_t)g.Hp;
+    const bool twin = nh2 >= 0;
+    const int nhb = twin ? nh2 : nh;
+    const double *rl = reinterpret_cast<const double *>(pick3(a.rl, sys));
+    double *v = reinterpret_cast<double *>(pick3(a.v, sys));
+    const double *lu = sys == 0 ? a.ldp : sys == 1 ? a.ldm : a.ldz;
+    if (pick3(a.ldpiv, sys))
+        solve_async2<true, 192>(lu, pick3(a.pivld, sys), g.N, g.Hp, nh, rl + 2 * (size_t)nh + part,
+                                rl + 2 * (size_t)nhb + part, st, v + 2 * (size_t)nh + part, v + 2 * (size_t)nhb + part,
+                                st, twin, ring4p + threadIdx.x);
+    else
+        solve_async2<false, 192>(lu, nullptr, g.N, g.Hp, nh, rl + 2 * (size_t)nh + part, rl + 2 * (size_t)nhb + part,
+                                 st, v + 2 * (size_t)nh + part, v + 2 * (size_t)nhb + part, st, twin,
+                                 ring4p + threadIdx.x);
+}
+
 // S2: warp = (re or im) of 32 consecutive modes
 __device__ __forceinline__ void solve_pnp_body(const StepArgs &a, int bx) {
     extern __shared__ double ring2[];
@@ -825,6 +1061,8 @@ __global__ void __launch_bounds__(64, 8) k_solve_pnp(StepArgs a) { solve_pnp_bod
 __global__ void k_step_proj(StepArgs a) { step_proj_body(a, blockIdx.x, blockIdx.y); }
 __global__ void __launch_bounds__(192, 4) k_solve_ld(StepArgs a) { solve_ld_body(a, blockIdx.x); }
 __global__ void __launch_bounds__(LDR_BT) k_solve_ldr(StepArgs a) { solve_ld_rebuild_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(64, 8) k_solve_pnp2(StepArgs a) { solve_pnp2_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(192, 3) k_solve_ld2(StepArgs a) { solve_ld2_body(a, blockIdx.x); }
 __global__ void __launch_bounds__(TM *TR) k_step_final(StepArgs a) { step_final_body(a, blockIdx.x); }
 
 #define PF_BATCH1(NAME, BODY, BOUNDS)                                                          \
@@ -836,6 +1074,8 @@ __global__ void __launch_bounds__(TM *TR) k_step_final(StepArgs a) { step_final_
 PF_BATCH1(k_solve_pnp_batch, solve_pnp_body, __launch_bounds__(64, 8))
 PF_BATCH1(k_solve_ld_batch, solve_ld_body, __launch_bounds__(192, 4))
 PF_BATCH1(k_solve_ldr_batch, solve_ld_rebuild_body, __launch_bounds__(LDR_BT))
+PF_BATCH1(k_solve_pnp2_batch, solve_pnp2_body, __launch_bounds__(64, 8))
+PF_BATCH1(k_solve_ld2_batch, solve_ld2_body, __launch_bounds__(192, 3))
 PF_BATCH1(k_step_final_batch, step_final_body, __launch_bounds__(TM *TR))
 #undef PF_BATCH1
 
@@ -908,6 +1148,16 @@ static bool ld_rebuild(const pf_ctx *ctx) {
     return !any_ld_pivoted(ctx) && ctx->g.N >= 2 * KL + 2 && ctx->tune.ld_solver == PF_LD_REBUILT;
 }
 
+// The streamed solves with modes k and -k paired on one factor stream
+// (pressure and Helmholtz); PF_LD_AUTO takes the built-in choice.
+static constexpr int LD_BUILTIN = PF_LD_STREAMED;
+static bool ld_paired(const pf_ctx *ctx) {
+    const int c = ctx->tune.ld_solver == PF_LD_AUTO ? LD_BUILTIN : ctx->tune.ld_solver;
+    return c == PF_LD_PAIRED;
+}
+static size_t ld2_smem(bool piv) { return (size_t)192 * RING * (piv ? KV + 1 : KL + 2) * sizeof(double); }
+static size_t pnp_smem() { return (size_t)64 * RING * (KV + 1) * sizeof(double); }
+
 static size_t rhs_smem(int N) { return (size_t)N * HM * sizeof(double2); }
 
 static int step_attrs() {
@@ -922,6 +1172,11 @@ static int step_attrs() {
         const int ldr = (int)ldr_smem(HR * 8);
         PF_CUDA(cudaFuncSetAttribute(k_solve_ldr, cudaFuncAttributeMaxDynamicSharedMemorySize, ldr));
         PF_CUDA(cudaFuncSetAttribute(k_solve_ldr_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, ldr));
+        PF_CUDA(cudaFuncSetAttribute(k_solve_ld2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ld2_smem(true)));
+        PF_CUDA(cudaFuncSetAttribute(k_solve_ld2_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)ld2_smem(true)));
+        PF_CUDA(cudaFuncSetAttribute(k_solve_pnp2, cudaFuncAttributeMaxDynamicSharedMemorySize, pnp));
+        PF_CUDA(cudaFuncSetAttribute(k_solve_pnp2_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, pnp));
         const int rhs = (int)rhs_smem(128);
         PF_CUDA(cudaFuncSetAttribute(k_step_rhs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, rhs));
         PF_CUDA(cudaFuncSetAttribute(k_step_rhs<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, rhs));
@@ -960,7 +1215,10 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
     PF_LAUNCHED(ctx);
     {
         ProfScope ps_(ctx, PF_K_PPE);
-        k_solve_pnp<<<tiles, 64, (size_t)64 * RING * (KV + 1) * sizeof(double), ctx->stream>>>(a);
+        if (ld_paired(ctx))
+            k_solve_pnp2<<<pair_tiles(g), 64, pnp_smem(), ctx->stream>>>(a);
+        else
+            k_solve_pnp<<<tiles, 64, pnp_smem(), ctx->stream>>>(a);
     }
     PF_LAUNCHED(ctx);
     {
@@ -972,6 +1230,8 @@ int pf_vel_step_fused(pf_ctx *ctx, int corrector) {
         ProfScope ps_(ctx, PF_K_LUSOLVE);
         if (ld_rebuild(ctx))
             k_solve_ldr<<<ldr_tiles(g), LDR_BT, ldr_smem(g.N), ctx->stream>>>(a);
+        else if (ld_paired(ctx))
+            k_solve_ld2<<<pair_tiles(g), 192, ld2_smem(any_ld_pivoted(ctx)), ctx->stream>>>(a);
         else
             k_solve_ld<<<tiles, 192, (size_t)192 * RING * ldsw * sizeof(double), ctx->stream>>>(a);
     }
@@ -996,6 +1256,12 @@ struct pf_step_batch {
     int nld[2];
     int2 *ldrmap;              // tiles of the pipes whose Helmholtz factors are rebuilt on chip
     int nldr, ldrN;            // their count and largest N
+    int2 *pmap;                // 32-item pair tiles of the pipes whose solves pair modes k and -k
+    int np2;
+    int2 *ld2map[2];           // the same tiles split by whether any Helmholtz factorisation [1] pivoted
+    int nld2[2];
+    int2 *pnpmap;              // 32-mode tiles of the other pipes (pressure solve)
+    int npnp;
     int maxN;
     bool anypiv;
 };
@@ -1009,6 +1275,10 @@ void pf_step_batch_free(pf_step_batch *b) {
     cudaFree(b->ldmap[0]);
     cudaFree(b->ldmap[1]);
     cudaFree(b->ldrmap);
+    cudaFree(b->pmap);
+    cudaFree(b->ld2map[0]);
+    cudaFree(b->ld2map[1]);
+    cudaFree(b->pnpmap);
     cudaFree(b->proj);
     delete b;
 }
@@ -1021,7 +1291,7 @@ int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
     b->maxN = 0;
     b->anypiv = false;
     std::vector<StepArgs> h(n);
-    std::vector<int2> tile, proj, half, ldm[2], ldr;
+    std::vector<int2> tile, proj, half, ldm[2], ldr, pm, ld2m[2], pnpm;
     b->ldrN = 0;
     for (int i = 0; i < n; ++i) {
         const Geo &g = pipes[i]->g;
@@ -1033,7 +1303,14 @@ int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
         b->maxN = std::max(b->maxN, g.N);
         b->anypiv |= any_ld_pivoted(pipes[i]);
         for (int t = 0; t < (int)grid1(g.H, TM); ++t) tile.push_back(make_int2(i, t));
-        if (ld_rebuild(pipes[i])) {
+        if (ld_paired(pipes[i])) {
+            for (int t = 0; t < pair_tiles(g); ++t) pm.push_back(make_int2(i, t));
+        } else {
+            for (int t = 0; t < (int)grid1(g.H, TM); ++t) pnpm.push_back(make_int2(i, t));
+        }
+        if (ld_paired(pipes[i])) {
+            for (int t = 0; t < pair_tiles(g); ++t) ld2m[any_ld_pivoted(pipes[i]) ? 1 : 0].push_back(make_int2(i, t));
+        } else if (ld_rebuild(pipes[i])) {
             for (int t = 0; t < ldr_tiles(g); ++t) ldr.push_back(make_int2(i, t));
             b->ldrN = std::max(b->ldrN, g.N);
         } else {
@@ -1069,10 +1346,14 @@ int pf_step_batch_build(pf_ctx *const *pipes, int n, pf_step_batch **out) {
             return PF_ERR_CUDA;
         }
     }
-    b->nldr = (int)ldr.size();
-    if (cudaMalloc((void **)&b->ldrmap, std::max<size_t>(1, ldr.size()) * sizeof(int2)) != cudaSuccess ||
-        (!ldr.empty() && cudaMemcpy(b->ldrmap, ldr.data(), ldr.size() * sizeof(int2), cudaMemcpyHostToDevice) !=
-                             cudaSuccess)) {
+    auto upload_map = [&](int2 **d, const std::vector<int2> &h, int *count) {
+        *count = (int)h.size();
+        return cudaMalloc((void **)d, std::max<size_t>(1, h.size()) * sizeof(int2)) == cudaSuccess &&
+               (h.empty() || cudaMemcpy(*d, h.data(), h.size() * sizeof(int2), cudaMemcpyHostToDevice) == cudaSuccess);
+    };
+    if (!upload_map(&b->ldrmap, ldr, &b->nldr) || !upload_map(&b->pmap, pm, &b->np2) ||
+        !upload_map(&b->ld2map[0], ld2m[0], &b->nld2[0]) || !upload_map(&b->ld2map[1], ld2m[1], &b->nld2[1]) ||
+        !upload_map(&b->pnpmap, pnpm, &b->npnp)) {
         pf_step_batch_free(b);
         pf_set_error("batched step: tile map upload failed");
         return PF_ERR_CUDA;
@@ -1112,7 +1393,8 @@ int pf_step_batch_launch(pf_step_batch *b, int state, int corrector, cudaStream_
     PF_CHECK_LAUNCH();
     {
         StageScope ss_(prof, PF_K_PPE, st);
-        k_solve_pnp_batch<<<b->ntile, 64, (size_t)64 * RING * (KV + 1) * sizeof(double), st>>>(a, b->tile);
+        if (b->npnp > 0) k_solve_pnp_batch<<<b->npnp, 64, pnp_smem(), st>>>(a, b->pnpmap);
+        if (b->np2 > 0) k_solve_pnp2_batch<<<b->np2, 64, pnp_smem(), st>>>(a, b->pmap);
     }
     PF_CHECK_LAUNCH();
     {
@@ -1129,6 +1411,8 @@ int pf_step_batch_launch(pf_step_batch *b, int state, int corrector, cudaStream_
                 k_solve_ld_batch<<<b->nld[q], 192, (size_t)192 * RING * (q ? KV + 1 : KL + 1) * sizeof(double), st>>>(
                     a, b->ldmap[q]);
         if (b->nldr > 0) k_solve_ldr_batch<<<b->nldr, LDR_BT, ldr_smem(b->ldrN), st>>>(a, b->ldrmap);
+        for (int q = 0; q < 2; ++q)
+            if (b->nld2[q] > 0) k_solve_ld2_batch<<<b->nld2[q], 192, ld2_smem(q == 1), st>>>(a, b->ld2map[q]);
     }
     PF_CHECK_LAUNCH();
     {
@@ -1136,6 +1420,7 @@ int pf_step_batch_launch(pf_step_batch *b, int state, int corrector, cudaStream_
         k_step_final_batch<<<b->ntile, TM * TR, 0, st>>>(a, b->tile);
     }
     PF_CHECK_LAUNCH();
-    *nk += 4 + (b->nld[0] > 0) + (b->nld[1] > 0) + (b->nldr > 0);
+    *nk += 3 + (b->npnp > 0) + (b->np2 > 0) + (b->nld[0] > 0) + (b->nld[1] > 0) + (b->nldr > 0) + (b->nld2[0] > 0) +
+           (b->nld2[1] > 0);
     return PF_OK;
 }

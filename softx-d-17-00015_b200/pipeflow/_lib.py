@@ -55,6 +55,7 @@ class pf_tim_state(C.Structure):
 PF_LD_AUTO = 0
 PF_LD_STREAMED = 1
 PF_LD_REBUILT = 2
+PF_LD_PAIRED = 3
 
 
 class pf_tuning(C.Structure):

@@ -20,7 +20,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .api import Pipe, PipeConfig, Server
+from .api import Pipe, PipeConfig, PipeflowError, Server
 from .ic import seeded_state
 
 
@@ -34,6 +34,7 @@ class Request:
     rid: int | None = None
     done_at: float | None = None
     result: list | None = field(default=None, repr=False)
+    error: str | None = None       # a failed request's message (the server reports it alone)
 
     @property
     def latency(self) -> float | None:
@@ -125,7 +126,10 @@ def run_stream(server: Server, reqs, keep_results: bool = False):
             now = time.perf_counter() - t0
             for rid in fin:
                 r = by_id[rid]
-                res = server.result(rid)
+                try:
+                    res = server.result(rid)
+                except PipeflowError as e:  # this request failed alone (e.g. its state went non-finite)
+                    res, r.error = None, str(e)
                 r.done_at = now
                 if keep_results:
                     r.result = res
@@ -138,4 +142,5 @@ def latency_summary(reqs) -> dict:
     steps = sum(r.nsteps for r in reqs)
     return {"requests": len(reqs), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()), "max_s": float(lat.max()), "pipe_steps": int(steps),
-            "krylov_requests": sum(r.kind == "krylov" for r in reqs)}
+            "krylov_requests": sum(r.kind == "krylov" for r in reqs),
+            "failed_requests": sum(r.error is not None for r in reqs)}

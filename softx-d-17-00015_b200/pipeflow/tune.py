@@ -4,9 +4,10 @@ No counterpart in the reference: its only tuning is FFTW's own plan search
 (FFTW_PATIENT, transform.fftw3.f90:36-57), which picks radices per transform
 length.  Here the choices are those pf_ctx_set_tuning exposes:
 
-  ld_solver  the Helmholtz banded solves stream the stored LU factors from
-             HBM (PF_LD_STREAMED, the built-in choice) or rebuild them on
-             chip (PF_LD_REBUILT, for factorisations that did not pivot);
+  ld_solver  the banded solves stream the stored LU factors from HBM
+             (PF_LD_STREAMED), pair the modes k and -k on one factor stream
+             (PF_LD_PAIRED), or rebuild the Helmholtz factors on chip
+             (PF_LD_REBUILT, for factorisations that did not pivot);
   nl_mc      columns (azimuthal modes m) per block of the z transform passes;
   nl_zc      z rows per block of the theta pass (two rows per complex FFT).
 
@@ -133,7 +134,7 @@ class Tuner:
             pipe.sync()
             return time.perf_counter() - t0
 
-        for knob, values in (("ld_solver", (L.PF_LD_AUTO, L.PF_LD_REBUILT)),
+        for knob, values in (("ld_solver", (L.PF_LD_AUTO, L.PF_LD_REBUILT, L.PF_LD_PAIRED)),
                              ("nl_mc", _mc_candidates(pipe.M)), ("nl_zc", ZC_CANDIDATES)):
             def apply(v, knob=knob):
                 pipe.set_tuning(**dict(cur, **{knob: v}))
@@ -173,7 +174,7 @@ class Tuner:
         order = sorted(shapes, key=lambda s: -s[0] * s[1] * s[2] * len(shapes[s]))
         for knob in ("ld_solver", "nl_mc", "nl_zc"):
             for s in order:
-                values = {"ld_solver": (L.PF_LD_AUTO, L.PF_LD_REBUILT), "nl_mc": _mc_candidates(s[2]),
+                values = {"ld_solver": (L.PF_LD_AUTO, L.PF_LD_REBUILT, L.PF_LD_PAIRED), "nl_mc": _mc_candidates(s[2]),
                           "nl_zc": ZC_CANDIDATES}[knob]
 
                 def apply(v, s=s, knob=knob):

@@ -31,15 +31,20 @@ def _pair(cfgd, **extra):
     return a, b
 
 
-@pytest.mark.parametrize("cfgd", [SMALL[0], SMALL[1], CFG1], ids=["small0", "small1", "cfg1"])
+PIVOTING = dict(N=64, K=4, M=4, Mp=1, Re=1900.0, alpha=1.2, dt=0.01)  # Helmholtz factors pivot
+
+
+@pytest.mark.parametrize("cfgd", [SMALL[0], SMALL[1], CFG1, PIVOTING], ids=["small0", "small1", "cfg1", "pivoting"])
 @pytest.mark.parametrize("mixed", [False, True], ids=["fp64", "mixed"])
-def test_helmholtz_factors_rebuilt_on_chip_equal_streamed(cfgd, mixed):
+@pytest.mark.parametrize("solver", ["rebuilt", "paired"])
+def test_helmholtz_solver_choices_equal_streamed(cfgd, mixed, solver):
     import pipeflow as P
     extra = {"precision": P.PF_PREC_MIXED} if mixed else {}
     a, b = _pair(cfgd, **extra)
-    a.set_tuning(ld_solver=P.PF_LD_REBUILT)
+    choice = P.PF_LD_REBUILT if solver == "rebuilt" else P.PF_LD_PAIRED
+    a.set_tuning(ld_solver=choice)
     b.set_tuning(ld_solver=P.PF_LD_STREAMED)
-    assert a.get_tuning()["ld_solver"] == P.PF_LD_REBUILT
+    assert a.get_tuning()["ld_solver"] == choice
     o = oracle_pipe(cfgd)
     o.vel_matrices()
     st = O.seeded_state(o, 3, 1e-3)

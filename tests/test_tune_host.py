@@ -1,0 +1,96 @@
+"""Host logic of the autotuner (pipeflow/tune.py) without a GPU: candidate
+tiles, shape keys, the JSON cache, and that a batch is tuned shape by shape
+with the fastest candidate kept and the states restored.  The timings come
+from a fake pipe whose step time depends on its launch choices."""
+import json
+
+import pipeflow as P
+from pipeflow import tune as T
+
+
+def test_tile_candidates_cover_the_built_in_and_the_whole_range():
+    for M in (4, 12, 24, 32, 48):
+        c = T._mc_candidates(M)
+        assert c[0] == 0 and M in c and all(1 <= x <= M for x in c[1:])
+        assert c == sorted(set(c))
+    assert 0 in T.ZC_CANDIDATES and all(z % 2 == 0 for z in T.ZC_CANDIDATES)
+
+
+class _Cfg:
+    def __init__(self, precision):
+        self.precision = precision
+
+
+class FakePipe:
+    """Stands in for pipeflow.Pipe: records its tuning and state, and makes
+    the tuner's clock advance by a cost that depends on the tuning."""
+
+    clock = [0.0]
+
+    def __init__(self, N, K, M, precision, best):
+        self.N, self.K, self.M, self.Mp = N, K, M, 1
+        self.cfg = _Cfg(precision)
+        self.best = best
+        self.tuning = {"ld_solver": 0, "nl_mc": 0, "nl_zc": 0}
+        self.state = [("s", N)]
+        self.steps = 0
+        self._tim = {"step": 0}
+
+    # the parts of Pipe the tuner uses
+    def set_tuning(self, ld_solver=0, nl_mc=0, nl_zc=0):
+        if nl_zc % 2:
+            raise P.PipeflowError(-1, "odd theta tile")
+        self.tuning = {"ld_solver": ld_solver, "nl_mc": nl_mc, "nl_zc": nl_zc}
+
+    def cost(self):
+        return sum(abs(self.tuning[k] - self.best[k]) for k in self.tuning) + 1.0
+
+    def get_state(self):
+        return list(self.state)
+
+    def set_state(self, *st):
+        self.state = list(st)
+
+    @property
+    def tim(self):
+        return dict(self._tim)
+
+    def set_tim(self, t):
+        self._tim = dict(t)
+
+
+class FakeBatch:
+    def __init__(self, pipes):
+        self.pipes = pipes
+
+    def step(self, n, orbit=False):
+        for p in self.pipes:
+            p.state = [("stepped", p.N)]
+            p._tim["step"] += n
+        FakePipe.clock[0] += n * sum(p.cost() for p in self.pipes)
+
+    def sync(self):
+        pass
+
+
+def test_batch_tuning_picks_each_shapes_fastest_choice_and_caches_it(tmp_path, monkeypatch):
+    monkeypatch.setattr(T.time, "perf_counter", lambda: FakePipe.clock[0])
+    best_a = {"ld_solver": P.PF_LD_REBUILT, "nl_mc": 6, "nl_zc": 8}
+    best_b = {"ld_solver": P.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 16}
+    pipes = [FakePipe(32, 16, 12, 1, best_a), FakePipe(32, 16, 12, 1, best_a), FakePipe(48, 32, 24, 0, best_b)]
+    batch = FakeBatch(pipes)
+    cache = tmp_path / "tuning.json"
+    tuner = T.Tuner(cache_path=cache, steps=2, reps=1)
+    choice = tuner.tune_batch(batch)
+    assert choice == {"N32K16M12Mp1mixed": best_a, "N48K32M24Mp1fp64": best_b}
+    assert [p.tuning for p in pipes] == [best_a, best_a, best_b]
+    # states and counters restored after the timed steps
+    assert all(p.state == [("s", p.N)] and p.tim == {"step": 0} for p in pipes)
+    data = json.loads(cache.read_text())
+    assert list(data.values()) == [choice]
+    # a second tuner reads the cache and times nothing
+    for p in pipes:
+        p.set_tuning()
+    again = T.Tuner(cache_path=cache, steps=2, reps=1)
+    assert again.tune_batch(batch) == choice and again.log == []
+    assert [p.tuning for p in pipes] == [best_a, best_a, best_b]
