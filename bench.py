@@ -610,7 +610,9 @@ def sustained_rate(args, P, S, local):
             srv.close()
             lat = S.latency_summary(reqs)
             row[f"window_{w:g}s"] = {"requests": lat["requests"], "p50_s": lat["p50_s"], "p99_s": lat["p99_s"],
-                                     "served_timesteps_per_s": lat["pipe_steps"] / makespan}
+                                     "offered_timesteps_per_s": lat["pipe_steps"] / w,
+                                     "served_timesteps_per_s": lat["pipe_steps"] / makespan,
+                                     "failed_requests": lat["failed_requests"]}
         a, b = row.get(f"window_{args.sustained_window:g}s"), row.get(f"window_{2 * args.sustained_window:g}s")
         row["flat"] = bool(a and b and b["p99_s"] <= 1.3 * a["p99_s"])
         trials.append(row)
@@ -643,7 +645,7 @@ def main():
     ap.add_argument("--serve-window", type=float, default=0.5)
     ap.add_argument("--no-serve", dest="with_serve", action="store_false")
     ap.add_argument("--no-sustained", dest="sustained", action="store_false")
-    ap.add_argument("--sustained-rates", type=float, nargs="+", default=[2.0, 4.0, 8.0, 16.0])
+    ap.add_argument("--sustained-rates", type=float, nargs="+", default=[2.0, 4.0, 8.0, 12.0, 16.0, 24.0, 32.0])
     ap.add_argument("--sustained-window", type=float, default=2.0)
     ap.add_argument("--no-tune", dest="tune", action="store_false")
     ap.add_argument("--ld-solver", default="auto", choices=["auto", "streamed", "rebuilt", "paired"])

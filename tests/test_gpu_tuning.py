@@ -1,9 +1,10 @@
 """Launch choices (pf_ctx_set_tuning) change the speed, never the numbers.
 
-The Helmholtz solves of the fused step either stream the banded LU factors
-that k_lu_factor stored (PF_LD_STREAMED, the built-in choice) or rebuild them
-on chip in the same order of operations (PF_LD_REBUILT, for factorisations
-that did not pivot);
+The banded solves of the fused step stream the LU factors that k_lu_factor
+stored (PF_LD_STREAMED, the built-in choice), or do so with modes k and -k on
+one thread (PF_LD_PAIRED), or rebuild the Helmholtz factors on chip in the
+same order of operations (PF_LD_REBUILT, for factorisations that did not
+pivot);
 the transform passes take any z-pass column tile and any even theta-pass row
 tile.  Each pair of pipes here starts from the same seeded state and must
 stay bitwise equal step after step, and one of them is held to the oracle.
@@ -41,7 +42,7 @@ def test_helmholtz_solver_choices_equal_streamed(cfgd, mixed, solver):
     import pipeflow as P
     extra = {"precision": P.PF_PREC_MIXED} if mixed else {}
     a, b = _pair(cfgd, **extra)
-    choice = P.PF_LD_REBUILT if solver == "rebuilt" else P.PF_LD_PAIRED
+    choice = {"rebuilt": P.PF_LD_REBUILT, "paired": P.PF_LD_PAIRED}[solver]
     a.set_tuning(ld_solver=choice)
     b.set_tuning(ld_solver=P.PF_LD_STREAMED)
     assert a.get_tuning()["ld_solver"] == choice
@@ -106,6 +107,27 @@ def _batch(cfgs):
     for i, p in enumerate(b.pipes):
         P.seeded_state(p, 40 + i, 1e-3)
     return b
+
+
+def test_batch_with_every_solver_choice_equals_streamed():
+    """A batch whose pipes take different solver choices (so every batched
+    solve launch runs, pivoting and not) steps bitwise like one that streams
+    the factors everywhere."""
+    import pipeflow as P
+    mix = [dict(SMALL[0]), dict(SMALL[1]), dict(CFG1, precision=P.PF_PREC_MIXED), dict(PIVOTING),
+           dict(SMALL[1], precision=P.PF_PREC_MIXED), dict(CFG1), dict(PIVOTING, Re=2100.0), dict(SMALL[0])]
+    choices = [P.PF_LD_REBUILT, P.PF_LD_PAIRED, P.PF_LD_PAIRED, P.PF_LD_REBUILT, P.PF_LD_REBUILT, P.PF_LD_AUTO,
+               P.PF_LD_PAIRED, P.PF_LD_STREAMED]
+    a, b = _batch(mix), _batch(mix)
+    for p, c in zip(a.pipes, choices):
+        p.set_tuning(ld_solver=c)
+    for p in b.pipes:
+        p.set_tuning(ld_solver=P.PF_LD_STREAMED)
+    for _ in range(2):
+        a.step(2)
+        b.step(2)
+        for pa, pb in zip(a.pipes, b.pipes):
+            assert _states_equal(pa, pb)
 
 
 def test_autotuned_batch_equals_untuned(tmp_path):
