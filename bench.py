@@ -390,10 +390,11 @@ def run_batched(args, torch, P, dist, world, rank, local):
     P.api._check(batch.lib.pf_batch_stream(batch.h, P.api.C.byref(h)))
     master = torch.cuda.ExternalStream(h.value)
     tuned = None
-    if args.ld_solver != "auto":  # one Helmholtz solver for every pipe (profiling)
-        ld = {"streamed": P.PF_LD_STREAMED, "rebuilt": P.PF_LD_REBUILT, "paired": P.PF_LD_PAIRED}[args.ld_solver]
+    if args.ld_solver != "auto" or args.nl_fused:  # one choice for every pipe (profiling)
+        ld = {"auto": P.PF_LD_AUTO, "streamed": P.PF_LD_STREAMED, "rebuilt": P.PF_LD_REBUILT,
+              "paired": P.PF_LD_PAIRED}[args.ld_solver]
         for p in batch.pipes:
-            p.set_tuning(ld_solver=ld)
+            p.set_tuning(ld_solver=ld, nl_fused=1 if args.nl_fused else 0)
     if args.tune:
         # the project's autotuner picks the launch choices per pipe shape by
         # timing whole batch steps (untimed here; states restored afterwards)
@@ -649,6 +650,8 @@ def main():
     ap.add_argument("--sustained-window", type=float, default=2.0)
     ap.add_argument("--no-tune", dest="tune", action="store_false")
     ap.add_argument("--ld-solver", default="auto", choices=["auto", "streamed", "rebuilt", "paired"])
+    ap.add_argument("--nl-fused", action="store_true",
+                    help="transforms of a radial point in one block for every pipe where built")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 

@@ -111,9 +111,17 @@ typedef struct {
     int ld_solver; /* PF_LD_* */
     int nl_mc;     /* z-pass columns per block (1..M; 0 = built-in) */
     int nl_zc;     /* theta-pass z rows per block (even, 2..32; 0 = built-in) */
+    int nl_fused;  /* 1: mixed precision, the transforms of one radial point
+                      in one block where that kernel is built and its plane
+                      fits (0 = built-in: three passes) */
 } pf_tuning;
 int pf_ctx_set_tuning(pf_ctx *ctx, const pf_tuning *t);
 int pf_ctx_get_tuning(const pf_ctx *ctx, pf_tuning *t);
+/* How the fused nonlinear terms run with the current tuning: *passes = 1
+ * (mixed precision, one block per radial point: z inverse, theta pass and z
+ * forward with the (m, z) plane in shared memory) or 3 (three launches with
+ * the plane in HBM). */
+int pf_nl_passes(const pf_ctx *ctx, int *passes);
 int pf_ctx_sync(pf_ctx *ctx);
 /* H = number of harmonics (i_H1+1), Z = 3K, Th = 3M. */
 int pf_ctx_dims(const pf_ctx *ctx, int *N, int *H, int *Z, int *Th);

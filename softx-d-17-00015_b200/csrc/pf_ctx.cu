@@ -306,6 +306,7 @@ extern "C" int pf_ctx_set_tuning(pf_ctx *ctx, const pf_tuning *t) {
     PF_ARG(t->ld_solver == PF_LD_AUTO || t->ld_solver == PF_LD_STREAMED || t->ld_solver == PF_LD_REBUILT ||
                t->ld_solver == PF_LD_PAIRED,
            "pf_ctx_set_tuning: bad ld_solver");
+    PF_ARG(t->nl_fused == 0 || t->nl_fused == 1, "pf_ctx_set_tuning: nl_fused is 0 or 1");
     PF_TRY(pf_nl_tiles_check(ctx, t));
     if (std::memcmp(&ctx->tune, t, sizeof(pf_tuning)) == 0) return PF_OK;
     PF_CUDA(cudaStreamSynchronize(ctx->stream));

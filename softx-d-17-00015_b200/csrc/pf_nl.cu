@@ -134,6 +134,30 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *p, double v) 
     atomicMax(p, (unsigned long long)__double_as_longlong(v));
 }
 
+// u x curl(u) (velocity.f90:325-329) of two packed physical rows (.x row za,
+// .y row zb), scaled for the forward transform; u = (u_r, u_t, u_z, curl)
+template <typename C, typename R>
+__device__ __forceinline__ void cross_scaled(const C (&u)[6], R scale, C &pr, C &pt, C &pz) {
+    pr = CTraits<C>::make((u[1].x * u[5].x - u[2].x * u[4].x) * scale, (u[1].y * u[5].y - u[2].y * u[4].y) * scale);
+    pt = CTraits<C>::make((u[2].x * u[3].x - u[0].x * u[5].x) * scale, (u[2].y * u[3].y - u[0].y * u[5].y) * scale);
+    pz = CTraits<C>::make((u[0].x * u[4].x - u[1].x * u[3].x) * scale, (u[0].y * u[4].y - u[1].y * u[3].y) * scale);
+}
+
+// the z-forward epilogue at one kept mode: the transformed product x plus
+// vel_addHPF's terms (velocity.f90:338-361); v = u_comp, vr = u_r there
+__device__ __forceinline__ double2 hpf_out(double2 o, int comp, double av, double b, double2 v, double2 vr,
+                                           bool pr0, double Pr0, double Re) {
+    if (comp == 2) {
+        o.x = o.x + av * v.y + b * vr.x;
+        o.y = o.y - av * v.x + b * vr.y;
+        if (pr0) o.x = o.x + 4.0 * Pr0 / Re;
+    } else {
+        o.x = o.x + av * v.y;
+        o.y = o.y - av * v.x;
+    }
+    return o;
+}
+
 template <int TL, typename C>
 __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
     using R = typename CTraits<C>::R;
@@ -186,19 +210,18 @@ __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) u[c] = phys[(c * np + zp) * RS + t];
         // .x holds row za, .y row zb
-        const C pr = CTraits<C>::make((u[1].x * u[5].x - u[2].x * u[4].x) * scale,
-                                      (u[1].y * u[5].y - u[2].y * u[4].y) * scale);
-        const C pt = CTraits<C>::make((u[2].x * u[3].x - u[0].x * u[5].x) * scale,
-                                      (u[2].y * u[3].y - u[0].y * u[5].y) * scale);
-        const C pz = CTraits<C>::make((u[0].x * u[4].x - u[1].x * u[3].x) * scale,
-                                      (u[0].y * u[4].y - u[1].y * u[3].y) * scale);
+        C pr, pt, pz;
+        cross_scaled(u, scale, pr, pt, pz);
         prod[(0 * np + zp) * RS + t] = pr;
         prod[(1 * np + zp) * RS + t] = pt;
         prod[(2 * np + zp) * RS + t] = pz;
-        const bool hasb = z0 + 2 * zp + 1 < Z;
-        mr = fmax(mr, fmax(fabs(u[0].x), hasb ? fabs(u[0].y) : (R)0));
-        mt = fmax(mt, fmax(fabs(u[1].x), hasb ? fabs(u[1].y) : (R)0));
-        mz = fmax(mz, fmax(fabs(u[2].x + base), hasb ? fabs(u[2].y + base) : (R)0));
+        // grid points only: a pair past Z (the last tile's padding) is no point
+        if (z0 + 2 * zp < Z) {
+            const bool hasb = z0 + 2 * zp + 1 < Z;
+            mr = fmax(mr, fmax(fabs(u[0].x), hasb ? fabs(u[0].y) : (R)0));
+            mt = fmax(mt, fmax(fabs(u[1].x), hasb ? fabs(u[1].y) : (R)0));
+            mz = fmax(mz, fmax(fabs(u[2].x + base), hasb ? fabs(u[2].y + base) : (R)0));
+        }
     }
     __shared__ double cflw[3][NL_THREADS / 32];  // warp maxima; three atomics per block
     if (a.cfl) {
@@ -279,18 +302,176 @@ __device__ __forceinline__ void nl_zfwd_body(const NLArgs &a, int bx, int by, in
         const int nh = m * (2 * K - 1) + kk;
         const C x = res[c * RS + (kk >= 0 ? kk : ZL + kk)];
         const double av = g.alpha * kk * U;
-        double2 o = make_double2((double)x.x, (double)x.y);
-        const double2 v = uc[nh];
-        if (comp == 2) {
-            const double2 vr = ur0[nh];
-            o.x = o.x + av * v.y + b * vr.x;
-            o.y = o.y - av * v.x + b * vr.y;
-            if (nh == 0 && a.const_flux) o.x = o.x + 4.0 * Pr0 / g.Re;
+        const double2 vr = comp == 2 ? ur0[nh] : make_double2(0.0, 0.0);
+        f[nh] = hpf_out(make_double2((double)x.x, (double)x.y), comp, av, b, uc[nh], vr, nh == 0 && a.const_flux,
+                        Pr0, g.Re);
+    }
+}
+
+// ------------------------------------------- one radial point in one block
+// Mixed precision (FP32 transforms): the z inverse, theta pass and z forward
+// of one radial point n run in one block with the (m, z) plane of all six
+// components held in shared memory, so the intermediate never leaves the
+// SM.  The arithmetic is the three-pass kernels' own (the same row FFTs on
+// the same data, the same product and epilogue), so the results are bitwise
+// theirs; only where the data waits between the passes differs.
+//   plane P[(c*M + m)*PZ + z]  six components x M rows of the z transform
+//   rows  Q[(c*np + zp)*PT + t] the theta rows of one chunk of ZC z rows
+// The block sees every z of its radial point, so it stores the CFL maxima
+// of n outright (no reset, no atomics).
+static constexpr int FUSED_THREADS = 512;
+
+// theta-row pitch: the four-step pitch made odd, so the gather's column
+// writes of consecutive z-row pairs fall in distinct banks
+__host__ __device__ constexpr int fused_tpitch(int L) { return fft4_pitch(L) | 1; }
+
+template <int ZL, int TL>
+__host__ __device__ constexpr size_t fused_smem(int M, int ZC) {
+    return ((size_t)6 * M * fft4_pitch(ZL) + (size_t)3 * ZC * fused_tpitch(TL) + 2 * ZL + 2 * TL) * sizeof(float2);
+}
+
+template <int ZL, int TL>
+__device__ __forceinline__ void nl_fused_body(const NLArgs &a, int n) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    constexpr int PZ = fft4_pitch(ZL), PT = fused_tpitch(TL);
+    const Geo &g = a.g;
+    const int K = g.K, M = g.M, Z = ZL;
+    const int ZC = a.ZC, np = ZC / 2;
+    float2 *P = reinterpret_cast<float2 *>(smraw);
+    float2 *Q = P + 6 * M * PZ;
+    float2 *twz = Q + 3 * ZC * PT, *twz2 = twz + ZL, *twt = twz2 + ZL, *twt2 = twt + TL;
+    fft4_tables<ZL>(twz, twz2, reinterpret_cast<const float2 *>(a.twz));
+    fft4_tables<TL>(twt, twt2, reinterpret_cast<const float2 *>(a.twt));
+    const size_t Hp = g.Hp, fs = (size_t)g.N * Hp;
+    // z inverse input: u, or the FP32 curl(u) of the mean-mode pass,
+    // zero-padded to ZL with the Hermitian fill of m = 0 (as k_nl_zinv)
+    const float inZ = 1.0f / ZL, inM = 1.0f / M;
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < 6 * M * ZL; idx += blockDim.x) {
+        const int r = fdiv(idx, ZL, inZ), j = idx - r * ZL;
+        const int comp = fdiv(r, M, inM), m = r - comp * M;
+        int nh = -1;
+        bool conj = false;
+        if (m == 0) {
+            if (j < K) nh = j;
+            else if (j >= 2 * K + 1) nh = ZL - j, conj = true;
         } else {
-            o.x = o.x + av * v.y;
-            o.y = o.y - av * v.x;
+            const int kk = j < K ? j : (j >= 2 * K + 1 ? j - ZL : K);
+            if (kk < K) nh = m * (2 * K - 1) + kk;
         }
-        f[nh] = o;
+        float2 v = make_float2(0.f, 0.f);
+        if (nh >= 0) {
+            const size_t at = (size_t)n * Hp + nh;
+            v = comp < 3 ? to_c<float2>(pick3(a.u, comp)[at]) : a.curlf[(comp - 3) * fs + at];
+            if (conj) v.y = -v.y;
+        }
+        P[r * PZ + j] = v;
+    }
+    __syncthreads();
+    fft4_rows<ZL, +1>(P, 6 * M, PZ, twz, twz2);
+    // theta pass, ZC z rows at a time (as k_nl_theta)
+    const float scale = (float)(1.0 / (double)(g.Z * g.Th));
+    const float base = (float)(1.0 - a.dm.rp[4 * g.N + n] * a.dm.rp[4 * g.N + n]);
+    float mr = 0, mt = 0, mz = 0;
+    const float inp = 1.0f / np, inT = 1.0f / TL;
+    for (int z0 = 0; z0 < Z; z0 += ZC) {
+        // the Hermitian extension of M theta modes of two z rows as one
+        // complex row, written entry by entry (zeros included)
+        for (int idx = threadIdx.x; idx < 6 * np * TL; idx += blockDim.x) {
+            const int rest = fdiv(idx, np, inp), zp = idx - rest * np;
+            const int comp = fdiv(rest, TL, inT), t = rest - comp * TL;
+            const int za = z0 + 2 * zp, zb = za + 1;
+            const int m = t < M ? t : (t > TL - M ? TL - t : -1);
+            float2 x = make_float2(0.f, 0.f);
+            if (m >= 0) {
+                const float2 *row = P + (comp * M + m) * PZ;
+                const float2 va = za < Z ? row[za] : make_float2(0.f, 0.f);
+                const float2 vb = zb < Z ? row[zb] : make_float2(0.f, 0.f);
+                if (m == 0) x = make_float2(va.x, vb.x);
+                else if (t == m) x = make_float2(va.x - vb.y, va.y + vb.x);
+                else x = make_float2(va.x + vb.y, -va.y + vb.x);
+            }
+            Q[(comp * np + zp) * PT + t] = x;
+        }
+        __syncthreads();
+        fft4_rows<TL, +1>(Q, 6 * np, PT, twt, twt2);
+        // u x curl(u) (velocity.f90:325-329) in place over the first three
+        // components' rows, scaled for the forward transform
+        for (int idx = threadIdx.x; idx < np * TL; idx += blockDim.x) {
+            const int zp = fdiv(idx, TL, inT), t = idx - zp * TL;
+            float2 u[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) u[c] = Q[(c * np + zp) * PT + t];
+            float2 pr, pt, pz;
+            cross_scaled(u, scale, pr, pt, pz);
+            Q[(0 * np + zp) * PT + t] = pr;
+            Q[(1 * np + zp) * PT + t] = pt;
+            Q[(2 * np + zp) * PT + t] = pz;
+            const int za = z0 + 2 * zp;
+            if (za < Z) {
+                const bool hasb = za + 1 < Z;
+                mr = fmaxf(mr, fmaxf(fabsf(u[0].x), hasb ? fabsf(u[0].y) : 0.f));
+                mt = fmaxf(mt, fmaxf(fabsf(u[1].x), hasb ? fabsf(u[1].y) : 0.f));
+                mz = fmaxf(mz, fmaxf(fabsf(u[2].x + base), hasb ? fabsf(u[2].y + base) : 0.f));
+            }
+        }
+        __syncthreads();
+        fft4_rows<TL, -1>(Q, 3 * np, PT, twt, twt2);
+        // separate the two packed real transforms, keep m < M, back into the
+        // plane rows of the first three components
+        for (int idx = threadIdx.x; idx < 3 * M * np; idx += blockDim.x) {
+            const int rest = fdiv(idx, np, inp), zp = idx - rest * np;
+            const int comp = fdiv(rest, M, inM), m = rest - comp * M;
+            const float2 *X = Q + (comp * np + zp) * PT;
+            const float2 A = X[m], B = X[(TL - m) % TL];
+            const int za = z0 + 2 * zp, zb = za + 1;
+            float2 *row = P + (comp * M + m) * PZ;
+            if (za < Z) row[za] = make_float2(0.5f * (A.x + B.x), 0.5f * (A.y - B.y));
+            if (zb < Z) row[zb] = make_float2(0.5f * (A.y + B.y), -0.5f * (A.x - B.x));
+        }
+        __syncthreads();
+    }
+    __shared__ float cflw[3][FUSED_THREADS / 32];
+    if (a.cfl) {
+        for (int o = 16; o > 0; o >>= 1) {
+            mr = fmaxf(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+            mt = fmaxf(mt, __shfl_xor_sync(0xffffffffu, mt, o));
+            mz = fmaxf(mz, __shfl_xor_sync(0xffffffffu, mz, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            cflw[0][threadIdx.x >> 5] = mr;
+            cflw[1][threadIdx.x >> 5] = mt;
+            cflw[2][threadIdx.x >> 5] = mz;
+        }
+    }
+    fft4_rows<ZL, -1>(P, 3 * M, PZ, twz, twz2);  // synchronises first: cflw is complete after it
+    if (a.cfl && threadIdx.x < 3) {
+        float v = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v = fmaxf(v, cflw[threadIdx.x][w]);
+        a.cfl[3 * n + threadIdx.x] = (unsigned long long)__double_as_longlong((double)v);
+    }
+    // truncation to |k| < K and vel_addHPF (as k_nl_zfwd)
+    const double U = a.dm.velU[n], b = -a.dm.velUp[n];
+    double Pr0 = 0.0;
+    if (a.const_flux) {
+        for (int j = 0; j <= KL; ++j) Pr0 += a.u[2][(size_t)(g.N - 1 - KL + j) * Hp].x * a.dm.dr1[1 * (KL + 1) + j];
+        Pr0 = Pr0 / (-2.0);
+        if (n == 0 && threadIdx.x == 0) a.sc->Pr0 = Pr0;
+    }
+    const double2 *__restrict__ ur0 = a.u[0] + (size_t)n * Hp;
+    const float ik = 1.0f / (2 * K - 1), inMH = 1.0f / (M * (2 * K - 1));
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < 3 * M * (2 * K - 1); idx += blockDim.x) {
+        const int comp = fdiv(idx, M * (2 * K - 1), inMH), rest = idx - comp * M * (2 * K - 1);
+        const int m = fdiv(rest, 2 * K - 1, ik), kk = rest - m * (2 * K - 1) - (K - 1);
+        if (m == 0 && kk < 0) continue;
+        const int nh = m * (2 * K - 1) + kk;
+        const float2 x = P[(comp * M + m) * PZ + (kk >= 0 ? kk : ZL + kk)];
+        const double av = g.alpha * kk * U;
+        const double2 vr = comp == 2 ? ur0[nh] : make_double2(0.0, 0.0);
+        pick3(a.N, comp)[(size_t)n * Hp + nh] =
+            hpf_out(make_double2((double)x.x, (double)x.y), comp, av, b, pick3(a.u, comp)[(size_t)n * Hp + nh], vr,
+                    nh == 0 && a.const_flux, Pr0, g.Re);
     }
 }
 
@@ -321,6 +502,10 @@ template <int ZL, typename C>
 __global__ void __launch_bounds__(NL_THREADS, (NLOcc<C, ZL>::zfwd)) k_nl_zfwd(NLArgs a) {
     nl_zfwd_body<ZL, C>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
+template <int ZL, int TL>
+__global__ void __launch_bounds__(FUSED_THREADS, 1) k_nl_fused(NLArgs a) {
+    nl_fused_body<ZL, TL>(a, blockIdx.x);
+}
 
 // ------------------------------------------------------------ dispatch
 #define PF_NL_LENGTHS(X) X(12) X(15) X(18) X(24) X(36) X(48) X(72) X(96) X(144) X(192) X(288) X(384)
@@ -337,6 +522,48 @@ static bool nl_length_ok(int L) {
 }
 
 bool pf_nl_fused_supported(const pf_ctx *ctx) { return nl_length_ok(ctx->g.Z) && nl_length_ok(ctx->g.Th); }
+static bool fused_plan(const Geo &g, const pf_tuning &tu, bool mixed, int *ZC, size_t *smem);
+
+extern "C" int pf_nl_passes(const pf_ctx *ctx, int *passes) {
+    PF_ARG(ctx && passes, "pf_nl_passes: null argument");
+    int zc = 0;
+    size_t sm = 0;
+    *passes = fused_plan(ctx->g, ctx->tune, ctx->cfg.precision == PF_PREC_MIXED, &zc, &sm) ? 1 : 3;
+    return PF_OK;
+}
+
+// (Z, Th) pairs the one-block-per-radial-point kernel is built for: the
+// batched mix's shapes whose six-component plane fits in shared memory,
+// config-1, and the small test shapes
+#define PF_NL_FUSED_PAIRS(X) \
+    X(12, 12) X(18, 15) X(15, 18) X(72, 48) X(48, 36) X(48, 72) X(48, 96) X(96, 36) X(96, 72) X(96, 96) X(192, 36)
+
+static size_t fused_smem_of(int Z, int Th, int M, int ZC) {
+#define PF_CASE(ZL, TL) \
+    if (Z == ZL && Th == TL) return fused_smem<ZL, TL>(M, ZC);
+    PF_NL_FUSED_PAIRS(PF_CASE)
+#undef PF_CASE
+    return 0;
+}
+static constexpr size_t FUSED_MAX_SMEM = 224 * 1024;  // below the 227 KB per block, with the static maxima
+
+// Whether a pipe's transforms run as one block per radial point, and the
+// theta chunk and shared memory they take there: a tuning that asks for it,
+// mixed precision, a built (Z, Th) pair and a plane that fits.  The built-in
+// choice is the three passes: on the 64-pipe mix the one-block kernel took
+// 1.23 ms per evaluation against 1.01 ms (one 16-warp block per SM at
+// 86-128 registers; the three passes keep many more warps resident, and the
+// stages are bound by latency and barriers, not by the plane's HBM traffic).
+static bool fused_plan(const Geo &g, const pf_tuning &tu, bool mixed, int *ZC, size_t *smem) {
+    if (!mixed || !tu.nl_fused || fused_smem_of(g.Z, g.Th, g.M, 2) == 0) return false;
+    int zc = tu.nl_zc > 0 ? tu.nl_zc : 16;
+    while (zc > 2 && fused_smem_of(g.Z, g.Th, g.M, zc) > FUSED_MAX_SMEM) zc -= 2;
+    const size_t sm = fused_smem_of(g.Z, g.Th, g.M, zc);
+    if (sm > FUSED_MAX_SMEM) return false;
+    *ZC = zc;
+    *smem = sm;
+    return true;
+}
 
 // shared-memory elements of B transform rows (plus tables) for a built length
 template <typename C> static int rows_elems(int L, int B) {
@@ -421,10 +648,12 @@ static NLArgs make_nl_args(pf_ctx *ctx) {
     a.curlf = mixed ? reinterpret_cast<float2 *>(ctx->T) + (size_t)6 * ctx->g.N * ctx->g.M * ctx->g.Z : nullptr;
     a.twz = mixed ? (const void *)ctx->twZf : (const void *)ctx->twZ;
     a.twt = mixed ? (const void *)ctx->twTf : (const void *)ctx->twT;
+    int fzc = 0;
+    size_t fsm = 0;
     if (mixed) {
         const NLTiles<float2> t = nl_tiles<float2>(ctx->g, ctx->tune);
         a.MC = t.MC;
-        a.ZC = t.ZC;
+        a.ZC = fused_plan(ctx->g, ctx->tune, true, &fzc, &fsm) ? fzc : t.ZC;
     } else {
         const NLTiles<double2> t = nl_tiles<double2>(ctx->g, ctx->tune);
         a.MC = t.MC;
@@ -444,6 +673,21 @@ template <typename K> static int raise_smem(K kernel, size_t bytes, size_t &cur)
 template <typename C>
 static int launch_nl(pf_ctx *ctx, const NLArgs &a) {
     const Geo &g = ctx->g;
+    int fzc = 0;
+    size_t fsm = 0;
+    if (fused_plan(g, ctx->tune, sizeof(C) == 8, &fzc, &fsm)) {
+        ProfScope ps_(ctx, PF_K_THFWD);
+#define PF_CASE(ZL, TL)                                                   \
+    if (g.Z == ZL && g.Th == TL) {                                        \
+        static size_t set_ = 0;                                           \
+        PF_TRY(raise_smem(k_nl_fused<ZL, TL>, fsm, set_));                \
+        k_nl_fused<ZL, TL><<<g.N, FUSED_THREADS, fsm, ctx->stream>>>(a);  \
+    }
+        PF_NL_FUSED_PAIRS(PF_CASE)
+#undef PF_CASE
+        PF_LAUNCHED(ctx);
+        return PF_OK;
+    }
     const NLTiles<C> t = nl_tiles<C>(g, ctx->tune);
     const dim3 gz((g.M + t.MC - 1) / t.MC, g.N, 6), gt((g.Z + t.ZC - 1) / t.ZC, g.N), gf((g.M + t.MC - 1) / t.MC, g.N, 3);
     switch (g.Z) {
@@ -668,6 +912,14 @@ __global__ void __launch_bounds__(NL_THREADS, (NLOcc<C, ZL>::zfwd)) k_nl_zfwd_b(
     nl_zfwd_body<ZL, C>(a, pb.y % gx, (pb.y / gx) % a.g.N, pb.y / (gx * a.g.N));
 }
 
+template <int ZL, int TL>
+__global__ void __launch_bounds__(FUSED_THREADS, 1) k_nl_fused_b(const NLArgs *__restrict__ args,
+                                                                const int2 *__restrict__ blk) {
+    const int2 pb = blk[blockIdx.x];
+    const NLArgs a = args[pb.x];
+    nl_fused_body<ZL, TL>(a, pb.y);
+}
+
 __global__ void __launch_bounds__(MEAN_THREADS) k_nl_mean64_part_batch(const NLArgs *__restrict__ args,
                                                                       const int2 *__restrict__ blk) {
     const int2 pb = blk[blockIdx.x];
@@ -701,6 +953,7 @@ struct NLGroup {
     int2 *blk;
     int nblk;
     size_t smem;
+    int Th;      // one-block-per-radial-point groups: (Z, Th) = (L, Th)
 };
 constexpr int NLB_STAGES = 3;   // zinv, theta, zfwd
 constexpr int NLB_MAXG = 24;    // (transform length, precision) pairs
@@ -715,6 +968,11 @@ struct pf_nl_batch {
     size_t mean_sm;
     cudaStream_t aux[NLB_MAXG];
     cudaEvent_t fork[NLB_STAGES], join[NLB_STAGES][NLB_MAXG];
+    // pipes whose transforms run one block per radial point, one group per
+    // (Z, Th): launched on streams of their own beside the three-pass stages
+    std::vector<NLGroup> fgroups;
+    cudaStream_t faux[NLB_MAXG];
+    cudaEvent_t ffork, fjoin[NLB_MAXG];
 };
 
 bool pf_nl_batch_supported(pf_ctx *const *pipes, int n) {
@@ -735,8 +993,13 @@ void pf_nl_batch_free(pf_nl_batch *b) {
     }
     cudaFree(b->mean_blk);
     cudaFree(b->fin_blk);
-    for (int k = 0; k < NLB_MAXG; ++k)
+    for (NLGroup &gr : b->fgroups) cudaFree(gr.blk);
+    if (b->ffork) cudaEventDestroy(b->ffork);
+    for (int k = 0; k < NLB_MAXG; ++k) {
         if (b->aux[k]) cudaStreamDestroy(b->aux[k]);
+        if (b->faux[k]) cudaStreamDestroy(b->faux[k]);
+        if (b->fjoin[k]) cudaEventDestroy(b->fjoin[k]);
+    }
     delete b;
 }
 
@@ -750,13 +1013,22 @@ static bool is_mixed(const pf_ctx *c) { return c->cfg.precision == PF_PREC_MIXED
 
 template <typename C> static NLTiles<C> tiles_of(const pf_ctx *c) { return nl_tiles<C>(c->g, c->tune); }
 
+static bool fused_of(const pf_ctx *c, int *ZC = nullptr, size_t *smem = nullptr) {
+    int zc = 0;
+    size_t sm = 0;
+    const bool f = fused_plan(c->g, c->tune, is_mixed(c), &zc, &sm);
+    if (ZC) *ZC = zc;
+    if (smem) *smem = sm;
+    return f;
+}
+
 // blocks of stage st for the pipes of one (length, precision) group
 template <typename C>
 static void nlb_group_map(int st, int L, bool mixed, pf_ctx *const *pipes, int n, std::vector<int2> &map,
                           size_t &smem) {
     for (int i = 0; i < n; ++i) {
         const Geo &g = pipes[i]->g;
-        if ((st == 1 ? g.Th : g.Z) != L || is_mixed(pipes[i]) != mixed) continue;
+        if ((st == 1 ? g.Th : g.Z) != L || is_mixed(pipes[i]) != mixed || fused_of(pipes[i])) continue;
         const NLTiles<C> t = tiles_of<C>(pipes[i]);
         int nb = 0;
         if (st == 0) nb = ((g.M + t.MC - 1) / t.MC) * g.N * 6;
@@ -772,6 +1044,7 @@ static int nlb_groups(pf_nl_batch *b, pf_ctx *const *pipes, int n) {
     for (int st = 0; st < NLB_STAGES; ++st) {
         std::vector<std::pair<int, int>> keys;  // (L, mixed)
         for (int i = 0; i < n; ++i) {
+            if (fused_of(pipes[i])) continue;
             const std::pair<int, int> k(st == 1 ? pipes[i]->g.Th : pipes[i]->g.Z, is_mixed(pipes[i]) ? 1 : 0);
             if (std::find(keys.begin(), keys.end(), k) == keys.end()) keys.push_back(k);
         }
@@ -785,8 +1058,33 @@ static int nlb_groups(pf_nl_batch *b, pf_ctx *const *pipes, int n) {
             size_t smem = 0;
             if (k.second) nlb_group_map<float2>(st, k.first, true, pipes, n, map, smem);
             else nlb_group_map<double2>(st, k.first, false, pipes, n, map, smem);
-            b->groups[st].push_back(NLGroup{k.first, k.second != 0, nullptr, (int)map.size(), smem});
+            b->groups[st].push_back(NLGroup{k.first, k.second != 0, nullptr, (int)map.size(), smem, 0});
             PF_TRY(upload(&b->groups[st].back().blk, map));
+        }
+    }
+    {  // one block per radial point: groups by (Z, Th), largest planes first
+        std::vector<std::pair<int, int>> keys;
+        for (int i = 0; i < n; ++i)
+            if (fused_of(pipes[i])) {
+                const std::pair<int, int> k(pipes[i]->g.Z, pipes[i]->g.Th);
+                if (std::find(keys.begin(), keys.end(), k) == keys.end()) keys.push_back(k);
+            }
+        std::sort(keys.begin(), keys.end(), std::greater<std::pair<int, int>>());
+        if ((int)keys.size() > NLB_MAXG) {
+            pf_set_error("batched transforms: too many (Z, Th) groups");
+            return PF_ERR_ARG;
+        }
+        for (const auto &k : keys) {
+            std::vector<int2> map;
+            size_t smem = 0;
+            for (int i = 0; i < n; ++i) {
+                size_t sm = 0;
+                if (pipes[i]->g.Z != k.first || pipes[i]->g.Th != k.second || !fused_of(pipes[i], nullptr, &sm)) continue;
+                for (int r = 0; r < pipes[i]->g.N; ++r) map.push_back(make_int2(i, r));
+                smem = std::max(smem, sm);
+            }
+            b->fgroups.push_back(NLGroup{k.first, true, nullptr, (int)map.size(), smem, k.second});
+            PF_TRY(upload(&b->fgroups.back().blk, map));
         }
     }
     std::vector<int2> mean, fin;
@@ -833,6 +1131,12 @@ int pf_nl_batch_build(pf_ctx *const *pipes, int n, pf_nl_batch **out) {
     }
     for (int k = 1; k < ng && s == PF_OK; ++k)
         if (cudaStreamCreateWithFlags(&b->aux[k], cudaStreamNonBlocking) != cudaSuccess) s = PF_ERR_CUDA;
+    if (s == PF_OK && !b->fgroups.empty() && cudaEventCreateWithFlags(&b->ffork, cudaEventDisableTiming) != cudaSuccess)
+        s = PF_ERR_CUDA;
+    for (size_t k = 0; k < b->fgroups.size() && s == PF_OK; ++k)
+        if (cudaStreamCreateWithFlags(&b->faux[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->fjoin[k], cudaEventDisableTiming) != cudaSuccess)
+            s = PF_ERR_CUDA;
     if (s != PF_OK) {
         if (s == PF_ERR_CUDA) pf_set_error("batched transforms: allocation failed");
         pf_nl_batch_free(b);
@@ -866,6 +1170,21 @@ template <typename C> static int nlb_group_launch(int st, const NLGroup &gr, con
     }
     PF_CHECK_LAUNCH();
     return PF_OK;
+}
+
+static int nlb_fused_launch(const NLGroup &gr, const NLArgs *args, cudaStream_t s) {
+#define PF_CASE(ZL, TL)                                                              \
+    if (gr.L == ZL && gr.Th == TL) {                                                 \
+        static size_t set_ = 0;                                                      \
+        PF_TRY(raise_smem(k_nl_fused_b<ZL, TL>, gr.smem, set_));                     \
+        k_nl_fused_b<ZL, TL><<<gr.nblk, FUSED_THREADS, gr.smem, s>>>(args, gr.blk);  \
+        PF_CHECK_LAUNCH();                                                           \
+        return PF_OK;                                                                \
+    }
+    PF_NL_FUSED_PAIRS(PF_CASE)
+#undef PF_CASE
+    pf_set_error("batched transforms: (Z, Th) = (%d, %d) not built as one block per radial point", gr.L, gr.Th);
+    return PF_ERR_ARG;
 }
 
 // one stage: the first group on st, the others forked onto auxiliary streams
@@ -903,6 +1222,17 @@ int pf_nl_batch_launch(pf_nl_batch *b, int state, cudaStream_t st, pf_stage_prof
         k_nl_mean64_part_batch<<<b->nmean, MEAN_THREADS, b->mean_sm, st>>>(args, b->mean_blk);
         PF_CHECK_LAUNCH();
         *nk += 1;
+        // the pipes done one block per radial point, beside the three passes
+        // of the others (they need the mean-mode pass's FP32 curl)
+        if (!b->fgroups.empty()) {
+            PF_CUDA(cudaEventRecord(b->ffork, st));
+            for (size_t k = 0; k < b->fgroups.size(); ++k) {
+                PF_CUDA(cudaStreamWaitEvent(b->faux[k], b->ffork, 0));
+                PF_TRY(nlb_fused_launch(b->fgroups[k], args, b->faux[k]));
+                PF_CUDA(cudaEventRecord(b->fjoin[k], b->faux[k]));
+                ++*nk;
+            }
+        }
     }
     for (int stage = 0; stage < NLB_STAGES; ++stage) {
         StageScope ss_(prof, cats[stage], st);
@@ -910,6 +1240,7 @@ int pf_nl_batch_launch(pf_nl_batch *b, int state, cudaStream_t st, pf_stage_prof
     }
     if (b->nmean > 0) {
         StageScope ss_(prof, PF_K_ZFWD, st);
+        for (size_t k = 0; k < b->fgroups.size(); ++k) PF_CUDA(cudaStreamWaitEvent(st, b->fjoin[k], 0));
         k_nl_mean64_fin_batch<<<b->nfin, 128, 0, st>>>(args, b->fin_blk);
         PF_CHECK_LAUNCH();
         *nk += 1;

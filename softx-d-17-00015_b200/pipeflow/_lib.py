@@ -59,7 +59,7 @@ PF_LD_PAIRED = 3
 
 
 class pf_tuning(C.Structure):
-    _fields_ = [("ld_solver", C.c_int), ("nl_mc", C.c_int), ("nl_zc", C.c_int)]
+    _fields_ = [("ld_solver", C.c_int), ("nl_mc", C.c_int), ("nl_zc", C.c_int), ("nl_fused", C.c_int)]
 
 
 P = C.c_void_p
@@ -79,6 +79,7 @@ _SIGS = {
     "pf_ctx_set_stream": [P, P],
     "pf_ctx_set_tuning": [P, C.POINTER(pf_tuning)],
     "pf_ctx_get_tuning": [P, C.POINTER(pf_tuning)],
+    "pf_nl_passes": [P, C.POINTER(C.c_int)],
     "pf_ctx_sync": [P],
     "pf_ctx_dims": [P, IP, IP, IP, IP],
     "pf_ctx_device_bytes": [P, C.POINTER(C.c_ulonglong)],

@@ -235,16 +235,24 @@ class Pipe:
             pass
 
     # ---------------- launch choices ----------------
-    def set_tuning(self, ld_solver: int = L.PF_LD_AUTO, nl_mc: int = 0, nl_zc: int = 0):
+    def set_tuning(self, ld_solver: int = L.PF_LD_AUTO, nl_mc: int = 0, nl_zc: int = 0, nl_fused: int = 0):
         """Launch choices of the fused step (pf_ctx_set_tuning); every choice
         gives the same numbers bit for bit, only the speed differs."""
-        t = L.pf_tuning(int(ld_solver), int(nl_mc), int(nl_zc))
+        t = L.pf_tuning(int(ld_solver), int(nl_mc), int(nl_zc), int(nl_fused))
         _check(self.lib.pf_ctx_set_tuning(self.ctx, C.byref(t)))
 
     def get_tuning(self) -> dict:
         t = L.pf_tuning()
         _check(self.lib.pf_ctx_get_tuning(self.ctx, C.byref(t)))
-        return {"ld_solver": t.ld_solver, "nl_mc": t.nl_mc, "nl_zc": t.nl_zc}
+        return {"ld_solver": t.ld_solver, "nl_mc": t.nl_mc, "nl_zc": t.nl_zc, "nl_fused": t.nl_fused}
+
+    @property
+    def nl_passes(self) -> int:
+        """1 when the nonlinear terms run as one block per radial point, 3
+        when they take the three-pass transforms (pf_nl_passes)."""
+        v = C.c_int()
+        _check(self.lib.pf_nl_passes(self.ctx, C.byref(v)))
+        return v.value
 
     # ---------------- fields ----------------
     def coll(self, re=None, im=None) -> Coll:

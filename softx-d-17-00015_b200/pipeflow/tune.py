@@ -8,14 +8,17 @@ length.  Here the choices are those pf_ctx_set_tuning exposes:
              (PF_LD_STREAMED), pair the modes k and -k on one factor stream
              (PF_LD_PAIRED), or rebuild the Helmholtz factors on chip
              (PF_LD_REBUILT, for factorisations that did not pivot);
-  nl_mc      columns (azimuthal modes m) per block of the z transform passes;
+  nl_fused   in mixed precision, the three-pass transforms (0) or those of
+             one radial point in one block (1);
+  nl_mc      columns (azimuthal modes m) per block of the z transform passes
+             (not timed where one block per radial point runs);
   nl_zc      z rows per block of the theta pass (two rows per complex FFT).
 
 Every choice gives the same numbers bit for bit, so the tuner only times
 them.  It times timesteps in the steporbit form (exactly one corrector per
 step, so every candidate does the same work), by coordinate descent: the
 solver first, then the z tile, then the theta tile, each with the others
-held.  A pipe is tuned on its own; a batch is tuned shape by shape (pipes of
+held (then the transform form, then the tiles).  A pipe is tuned on its own; a batch is tuned shape by shape (pipes of
 one (N, K, M, Mp, precision) share a choice) while the whole batch steps,
 since the kernels of different shapes share the GPU.  Choices are cached in
 a JSON file (PIPEFLOW_TUNE_CACHE, default ~/.cache/pipeflow_b200/tuning.json)
@@ -35,6 +38,25 @@ from . import _lib as L
 from .api import PipeflowError
 
 ZC_CANDIDATES = (0, 4, 8, 16, 32)
+LD_CANDIDATES = (L.PF_LD_AUTO, L.PF_LD_REBUILT, L.PF_LD_PAIRED)
+KNOBS = ("ld_solver", "nl_fused", "nl_mc", "nl_zc")
+DEFAULT = {"ld_solver": L.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 0, "nl_fused": 0}
+
+
+def _candidates(knob: str, shape) -> tuple:
+    if knob == "ld_solver":
+        return LD_CANDIDATES
+    if knob == "nl_fused":
+        return (0, 1) if shape[4] == L.PF_PREC_MIXED else (0,)
+    if knob == "nl_mc":
+        return tuple(_mc_candidates(shape[2]))
+    return ZC_CANDIDATES
+
+
+def _one_pass(pipe) -> bool:
+    """Whether the pipe's nonlinear terms run as one block per radial point
+    with its current choices (the z-pass tile is then unused)."""
+    return getattr(pipe, "nl_passes", 3) == 1
 
 
 def _mc_candidates(M: int):
@@ -124,7 +146,7 @@ class Tuner:
                 pipe.set_tuning(**hit)
                 return hit
         snap = _Snapshot([pipe])
-        cur = {"ld_solver": L.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 0}
+        cur = dict(DEFAULT)
 
         def run():
             pipe.steporbit(2)
@@ -134,12 +156,13 @@ class Tuner:
             pipe.sync()
             return time.perf_counter() - t0
 
-        for knob, values in (("ld_solver", (L.PF_LD_AUTO, L.PF_LD_REBUILT, L.PF_LD_PAIRED)),
-                             ("nl_mc", _mc_candidates(pipe.M)), ("nl_zc", ZC_CANDIDATES)):
+        for knob in KNOBS:
+            if knob == "nl_mc" and _one_pass(pipe):
+                continue
             def apply(v, knob=knob):
                 pipe.set_tuning(**dict(cur, **{knob: v}))
                 cur[knob] = v
-            self._best(values, apply, run)
+            self._best(_candidates(knob, shape_of(pipe)), apply, run)
         snap.restore()
         self._store(key, dict(cur))
         return dict(cur)
@@ -160,7 +183,7 @@ class Tuner:
                         p.set_tuning(**hit[_shape_key(s)])
                 return hit
         snap = _Snapshot(batch.pipes)
-        choice = {s: {"ld_solver": L.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 0} for s in shapes}
+        choice = {s: dict(DEFAULT) for s in shapes}
 
         def run():
             batch.step(3, orbit=True)  # rebuild after a change: direct step, capture, replay
@@ -172,10 +195,11 @@ class Tuner:
 
         # largest shapes first: they carry most of the step
         order = sorted(shapes, key=lambda s: -s[0] * s[1] * s[2] * len(shapes[s]))
-        for knob in ("ld_solver", "nl_mc", "nl_zc"):
+        for knob in KNOBS:
             for s in order:
-                values = {"ld_solver": (L.PF_LD_AUTO, L.PF_LD_REBUILT, L.PF_LD_PAIRED), "nl_mc": _mc_candidates(s[2]),
-                          "nl_zc": ZC_CANDIDATES}[knob]
+                if knob == "nl_mc" and _one_pass(shapes[s][0]):
+                    continue
+                values = _candidates(knob, s)
 
                 def apply(v, s=s, knob=knob):
                     new = dict(choice[s], **{knob: v})

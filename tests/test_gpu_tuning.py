@@ -95,9 +95,11 @@ def test_tuning_rejects_bad_choices():
         g.set_tuning(nl_zc=3)
     with pytest.raises(Exception):
         g.set_tuning(ld_solver=7)
-    g.set_tuning(ld_solver=P.PF_LD_REBUILT)
+    with pytest.raises(Exception):
+        g.set_tuning(nl_fused=2)
+    g.set_tuning(ld_solver=P.PF_LD_REBUILT, nl_fused=1)
     g.set_tuning()
-    assert g.get_tuning() == {"ld_solver": P.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 0}
+    assert g.get_tuning() == {"ld_solver": P.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 0, "nl_fused": 0}
 
 
 def _batch(cfgs):
@@ -163,3 +165,77 @@ def test_autotuned_pipe_equals_untuned(tmp_path):
         a.timestep()
         b.timestep()
     assert _states_equal(a, b)
+
+
+MIXED_IDS = ["small0", "small1", "small2", "cfg1"]
+
+
+@pytest.mark.parametrize("cfgd", [SMALL[0], SMALL[1], SMALL[2], CFG1], ids=MIXED_IDS)
+def test_one_block_per_radial_point_equals_three_passes(cfgd):
+    """Mixed precision: the transforms of a radial point in one block (plane
+    in shared memory) give bitwise the three-pass kernels' states."""
+    import pipeflow as P
+    a, b = _pair(cfgd, precision=P.PF_PREC_MIXED)
+    a.set_tuning(nl_fused=1)
+    assert a.nl_passes == 1 and b.nl_passes == 3
+    st = O.seeded_state(oracle_pipe(cfgd), 5, 1e-3)
+    for g in (a, b):
+        state_to_dev(g, st)
+    for _ in range(4):
+        assert a.timestep() == b.timestep()
+        assert _states_equal(a, b)
+    a.steporbit(2)
+    b.steporbit(2)
+    assert _states_equal(a, b)
+
+
+def test_one_block_per_radial_point_cfl_maxima_drive_the_same_dt():
+    """Adaptive dt in mixed precision at config-1 (Z = 72: the last theta
+    chunk of 16 z rows is half padding): the CFL maxima the one-block kernel
+    stores outright equal the three-pass kernels' atomic maxima, so dt
+    follows the same sequence."""
+    import pipeflow as P
+    cfgd = dict(CFG1, dt=-1.0, maxdt=0.01, courant=0.5)
+    a, b = device_pipe(cfgd, precision=P.PF_PREC_MIXED), device_pipe(cfgd, precision=P.PF_PREC_MIXED)
+    a.set_tuning(nl_fused=1)
+    st = O.seeded_state(oracle_pipe(CFG1), 11, 1e-2)
+    for g in (a, b):
+        t = g.tim
+        t.dt = 0.004
+        g.set_tim(t)
+        g.vel_matrices()
+        state_to_dev(g, st)
+    dts = [a.tim.dt]
+    for _ in range(6):
+        assert a.timestep() == b.timestep()
+        assert a.tim.dt == b.tim.dt
+        assert _states_equal(a, b)
+        dts.append(a.tim.dt)
+    assert len(set(dts)) > 1
+
+
+def test_batched_one_block_per_radial_point_equals_three_passes():
+    """A batch whose mixed-precision pipes take the one-block kernel (several
+    (Z, Th) groups on their own streams, beside a pipe whose plane does not
+    fit and an FP64 pipe, which take the three passes) steps bitwise like the
+    same batch with every pipe on the three passes."""
+    import pipeflow as P
+    mx = P.PF_PREC_MIXED
+    base = dict(Mp=1, Re=2200.0, alpha=1.1, dt=0.01)
+    mix = [dict(base, N=32, K=16, M=12, precision=mx), dict(base, N=24, K=32, M=24, precision=mx),
+           dict(base, N=20, K=64, M=12, precision=mx), dict(base, N=16, K=64, M=24, precision=mx),
+           dict(CFG1, precision=mx), dict(SMALL[0]), dict(base, N=32, K=16, M=12, precision=mx)]
+    a, b = _batch(mix), _batch(mix)
+    for p in a.pipes:
+        p.set_tuning(nl_fused=1)
+    assert [p.nl_passes for p in a.pipes] == [1, 1, 1, 3, 1, 3, 1]
+    assert all(p.nl_passes == 3 for p in b.pipes)
+    for _ in range(2):
+        a.step(2)
+        b.step(2)
+        for pa, pb in zip(a.pipes, b.pipes):
+            assert _states_equal(pa, pb)
+    a.step(2, orbit=True)
+    b.step(2, orbit=True)
+    for pa, pb in zip(a.pipes, b.pipes):
+        assert _states_equal(pa, pb)

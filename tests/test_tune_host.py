@@ -31,16 +31,16 @@ class FakePipe:
         self.N, self.K, self.M, self.Mp = N, K, M, 1
         self.cfg = _Cfg(precision)
         self.best = best
-        self.tuning = {"ld_solver": 0, "nl_mc": 0, "nl_zc": 0}
+        self.tuning = {"ld_solver": 0, "nl_mc": 0, "nl_zc": 0, "nl_fused": 0}
         self.state = [("s", N)]
         self.steps = 0
         self._tim = {"step": 0}
 
     # the parts of Pipe the tuner uses
-    def set_tuning(self, ld_solver=0, nl_mc=0, nl_zc=0):
+    def set_tuning(self, ld_solver=0, nl_mc=0, nl_zc=0, nl_fused=0):
         if nl_zc % 2:
             raise P.PipeflowError(-1, "odd theta tile")
-        self.tuning = {"ld_solver": ld_solver, "nl_mc": nl_mc, "nl_zc": nl_zc}
+        self.tuning = {"ld_solver": ld_solver, "nl_mc": nl_mc, "nl_zc": nl_zc, "nl_fused": nl_fused}
 
     def cost(self):
         return sum(abs(self.tuning[k] - self.best[k]) for k in self.tuning) + 1.0
@@ -73,10 +73,19 @@ class FakeBatch:
         pass
 
 
+def test_split_is_only_tried_in_mixed_precision_and_the_one_pass_kernel_skips_the_z_tile():
+    assert T._candidates("nl_fused", (32, 16, 12, 1, P.PF_PREC_MIXED)) == (0, 1)
+    assert T._candidates("nl_fused", (32, 16, 12, 1, P.PF_PREC_FP64)) == (0,)
+
+    class OnePass:
+        nl_passes = 1
+    assert T._one_pass(OnePass()) and not T._one_pass(object())
+
+
 def test_batch_tuning_picks_each_shapes_fastest_choice_and_caches_it(tmp_path, monkeypatch):
     monkeypatch.setattr(T.time, "perf_counter", lambda: FakePipe.clock[0])
-    best_a = {"ld_solver": P.PF_LD_REBUILT, "nl_mc": 6, "nl_zc": 8}
-    best_b = {"ld_solver": P.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 16}
+    best_a = {"ld_solver": P.PF_LD_REBUILT, "nl_mc": 6, "nl_zc": 8, "nl_fused": 1}
+    best_b = {"ld_solver": P.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 16, "nl_fused": 0}
     pipes = [FakePipe(32, 16, 12, 1, best_a), FakePipe(32, 16, 12, 1, best_a), FakePipe(48, 32, 24, 0, best_b)]
     batch = FakeBatch(pipes)
     cache = tmp_path / "tuning.json"
