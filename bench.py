@@ -392,7 +392,7 @@ def run_batched(args, torch, P, dist, world, rank, local):
     tuned = None
     if args.ld_solver != "auto" or args.nl_fused:  # one choice for every pipe (profiling)
         ld = {"auto": P.PF_LD_AUTO, "streamed": P.PF_LD_STREAMED, "rebuilt": P.PF_LD_REBUILT,
-              "paired": P.PF_LD_PAIRED}[args.ld_solver]
+              "paired": P.PF_LD_PAIRED, "warpring": P.PF_LD_WARPRING}[args.ld_solver]
         for p in batch.pipes:
             p.set_tuning(ld_solver=ld, nl_fused=1 if args.nl_fused else 0)
     if args.tune:
@@ -490,6 +490,8 @@ def run_batched(args, torch, P, dist, world, rank, local):
                  "note": "flops by the 5 L log2 L count per complex FFT of length L; the FP32 peak is the nominal "
                          "148 SMs x 128 lanes x 2 x 1.965 GHz (not measured)"},
              "batch_step_ms": ms / args.steps,
+             # per-category stage spans of the warm-up steps (every category's event nodes on)
+             "stage_spans_us": {k: 1e3 * v[0] / v[1] for k, v in prof.items() if v[1] > 0},
              "step_roofline": {"bound": "hbm", "scope": "whole batch step (all stages, all pipes)",
                                "achieved": step_bytes / (ms / args.steps / 1e3) / 1e9, "unit": "GB/s"}}
     if rank == 0:
@@ -649,7 +651,7 @@ def main():
     ap.add_argument("--sustained-rates", type=float, nargs="+", default=[2.0, 4.0, 8.0, 12.0, 16.0, 24.0, 32.0])
     ap.add_argument("--sustained-window", type=float, default=2.0)
     ap.add_argument("--no-tune", dest="tune", action="store_false")
-    ap.add_argument("--ld-solver", default="auto", choices=["auto", "streamed", "rebuilt", "paired"])
+    ap.add_argument("--ld-solver", default="auto", choices=["auto", "streamed", "rebuilt", "paired", "warpring"])
     ap.add_argument("--nl-fused", action="store_true",
                     help="transforms of a radial point in one block for every pipe where built")
     args = ap.parse_args()

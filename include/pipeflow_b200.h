@@ -107,6 +107,10 @@ int pf_ctx_set_stream(pf_ctx *ctx, void *cuda_stream);
                              that did not pivot, N >= 10; else streamed) */
 #define PF_LD_PAIRED   3  /* streamed factors, modes k and -k paired on one
                              factor stream (pressure and Helmholtz solves) */
+#define PF_LD_WARPRING 4  /* streamed Helmholtz factors, one shared-memory ring
+                             per mode read by its real and imaginary lanes (the
+                             pressure solve does so for every choice but
+                             PF_LD_PAIRED) */
 typedef struct {
     int ld_solver; /* PF_LD_* */
     int nl_mc;     /* z-pass columns per block (1..M; 0 = built-in) */

@@ -304,7 +304,7 @@ extern "C" int pf_ctx_set_stream(pf_ctx *ctx, void *stream) {
 extern "C" int pf_ctx_set_tuning(pf_ctx *ctx, const pf_tuning *t) {
     PF_ARG(ctx && t, "pf_ctx_set_tuning: null argument");
     PF_ARG(t->ld_solver == PF_LD_AUTO || t->ld_solver == PF_LD_STREAMED || t->ld_solver == PF_LD_REBUILT ||
-               t->ld_solver == PF_LD_PAIRED,
+               t->ld_solver == PF_LD_PAIRED || t->ld_solver == PF_LD_WARPRING,
            "pf_ctx_set_tuning: bad ld_solver");
     PF_ARG(t->nl_fused == 0 || t->nl_fused == 1, "pf_ctx_set_tuning: nl_fused is 0 or 1");
     PF_TRY(pf_nl_tiles_check(ctx, t));

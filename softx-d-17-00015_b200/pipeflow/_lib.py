@@ -56,6 +56,7 @@ PF_LD_AUTO = 0
 PF_LD_STREAMED = 1
 PF_LD_REBUILT = 2
 PF_LD_PAIRED = 3
+PF_LD_WARPRING = 4
 
 
 class pf_tuning(C.Structure):

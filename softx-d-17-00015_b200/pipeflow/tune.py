@@ -5,9 +5,11 @@ No counterpart in the reference: its only tuning is FFTW's own plan search
 length.  Here the choices are those pf_ctx_set_tuning exposes:
 
   ld_solver  the banded solves stream the stored LU factors from HBM
-             (PF_LD_STREAMED), pair the modes k and -k on one factor stream
-             (PF_LD_PAIRED), or rebuild the Helmholtz factors on chip
-             (PF_LD_REBUILT, for factorisations that did not pivot);
+             (PF_LD_STREAMED), share the Helmholtz rings of a mode between
+             its real and imaginary lanes (PF_LD_WARPRING), pair the modes k
+             and -k on one factor stream (PF_LD_PAIRED), or rebuild the
+             Helmholtz factors on chip (PF_LD_REBUILT, for factorisations
+             that did not pivot);
   nl_fused   in mixed precision, the three-pass transforms (0) or those of
              one radial point in one block (1);
   nl_mc      columns (azimuthal modes m) per block of the z transform passes
@@ -38,7 +40,7 @@ from . import _lib as L
 from .api import PipeflowError
 
 ZC_CANDIDATES = (0, 4, 8, 16, 32)
-LD_CANDIDATES = (L.PF_LD_AUTO, L.PF_LD_REBUILT, L.PF_LD_PAIRED)
+LD_CANDIDATES = (L.PF_LD_AUTO, L.PF_LD_WARPRING, L.PF_LD_REBUILT, L.PF_LD_PAIRED)
 KNOBS = ("ld_solver", "nl_fused", "nl_mc", "nl_zc")
 DEFAULT = {"ld_solver": L.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 0, "nl_fused": 0}
 
@@ -51,6 +53,17 @@ def _candidates(knob: str, shape) -> tuple:
     if knob == "nl_mc":
         return tuple(_mc_candidates(shape[2]))
     return ZC_CANDIDATES
+
+
+def _fused_applies(pipe, cur: dict) -> bool:
+    """Whether asking for one block per radial point changes anything for
+    this pipe (mixed precision, a built (Z, Th) pair, a plane that fits)."""
+    if not hasattr(pipe, "nl_passes"):
+        return True
+    pipe.set_tuning(**dict(cur, nl_fused=1))
+    ok = pipe.nl_passes == 1
+    pipe.set_tuning(**cur)
+    return ok
 
 
 def _one_pass(pipe) -> bool:
@@ -157,7 +170,7 @@ class Tuner:
             return time.perf_counter() - t0
 
         for knob in KNOBS:
-            if knob == "nl_mc" and _one_pass(pipe):
+            if (knob == "nl_mc" and _one_pass(pipe)) or (knob == "nl_fused" and not _fused_applies(pipe, cur)):
                 continue
             def apply(v, knob=knob):
                 pipe.set_tuning(**dict(cur, **{knob: v}))
@@ -198,6 +211,8 @@ class Tuner:
         for knob in KNOBS:
             for s in order:
                 if knob == "nl_mc" and _one_pass(shapes[s][0]):
+                    continue
+                if knob == "nl_fused" and not _fused_applies(shapes[s][0], choice[s]):
                     continue
                 values = _candidates(knob, s)
 

@@ -37,12 +37,12 @@ PIVOTING = dict(N=64, K=4, M=4, Mp=1, Re=1900.0, alpha=1.2, dt=0.01)  # Helmholt
 
 @pytest.mark.parametrize("cfgd", [SMALL[0], SMALL[1], CFG1, PIVOTING], ids=["small0", "small1", "cfg1", "pivoting"])
 @pytest.mark.parametrize("mixed", [False, True], ids=["fp64", "mixed"])
-@pytest.mark.parametrize("solver", ["rebuilt", "paired"])
+@pytest.mark.parametrize("solver", ["rebuilt", "paired", "warpring"])
 def test_helmholtz_solver_choices_equal_streamed(cfgd, mixed, solver):
     import pipeflow as P
     extra = {"precision": P.PF_PREC_MIXED} if mixed else {}
     a, b = _pair(cfgd, **extra)
-    choice = {"rebuilt": P.PF_LD_REBUILT, "paired": P.PF_LD_PAIRED}[solver]
+    choice = {"rebuilt": P.PF_LD_REBUILT, "paired": P.PF_LD_PAIRED, "warpring": P.PF_LD_WARPRING}[solver]
     a.set_tuning(ld_solver=choice)
     b.set_tuning(ld_solver=P.PF_LD_STREAMED)
     assert a.get_tuning()["ld_solver"] == choice
@@ -118,7 +118,7 @@ def test_batch_with_every_solver_choice_equals_streamed():
     import pipeflow as P
     mix = [dict(SMALL[0]), dict(SMALL[1]), dict(CFG1, precision=P.PF_PREC_MIXED), dict(PIVOTING),
            dict(SMALL[1], precision=P.PF_PREC_MIXED), dict(CFG1), dict(PIVOTING, Re=2100.0), dict(SMALL[0])]
-    choices = [P.PF_LD_REBUILT, P.PF_LD_PAIRED, P.PF_LD_PAIRED, P.PF_LD_REBUILT, P.PF_LD_REBUILT, P.PF_LD_AUTO,
+    choices = [P.PF_LD_WARPRING, P.PF_LD_PAIRED, P.PF_LD_WARPRING, P.PF_LD_WARPRING, P.PF_LD_REBUILT, P.PF_LD_AUTO,
                P.PF_LD_PAIRED, P.PF_LD_STREAMED]
     a, b = _batch(mix), _batch(mix)
     for p, c in zip(a.pipes, choices):
