@@ -176,10 +176,10 @@ __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
     C *tw = bufA + (FR::smem_elems(rowsA) - 2 * TL), *tw2 = tw + TL;
     const int n = by, z0 = bx * ZC;
     fft4_tables<TL>(tw, tw2, twt);
-    for (int i = threadIdx.x; i < rowsA * RS; i += blockDim.x) bufA[i] = CTraits<C>::make(0, 0);
-    __syncthreads();
     // Hermitian-extend the M retained theta modes of two z rows into one
-    // complex row: X = a + i b (c2r ignores the DC imaginary parts)
+    // complex row: X = a + i b (c2r ignores the DC imaginary parts).  With
+    // TL = 3M every entry is written once: X[m] and X[TL-m] by mode m's
+    // thread, which also clears X[M+m] of the zero band (and m = 0 X[2M])
     const float inp = 1.0f / np, inM = 1.0f / M;
 #pragma unroll 4
     for (int idx = threadIdx.x; idx < 6 * M * np; idx += blockDim.x) {
@@ -190,8 +190,10 @@ __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
         const C va = (za < Z) ? col[za] : CTraits<C>::make(0, 0);
         const C vb = (zb < Z) ? col[zb] : CTraits<C>::make(0, 0);
         C *X = bufA + (comp * np + zp) * RS;
+        X[M + m] = CTraits<C>::make(0, 0);
         if (m == 0) {
             X[0] = CTraits<C>::make(va.x, vb.x);
+            X[2 * M] = CTraits<C>::make(0, 0);
         } else {
             X[m] = CTraits<C>::make(va.x - vb.y, va.y + vb.x);
             X[TL - m] = CTraits<C>::make(va.x + vb.y, -va.y + vb.x);
