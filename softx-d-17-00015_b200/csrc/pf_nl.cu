@@ -158,6 +158,14 @@ __device__ __forceinline__ double2 hpf_out(double2 o, int comp, double av, doubl
     return o;
 }
 
+// Whether the z-row pair (za, zb = za + 1) of an (m, z) column moves as one
+// 16-byte access: FP32 values, an even Z (every column then starts on a
+// 16-byte boundary and za, a tile start plus twice the pair index, is even)
+// and both rows inside the column.
+template <typename C> __device__ __forceinline__ bool pair16(int Z, int zb) {
+    return sizeof(C) == 8 && (Z & 1) == 0 && zb < Z;
+}
+
 template <int TL, typename C>
 __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
     using R = typename CTraits<C>::R;
@@ -187,8 +195,15 @@ __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
         const int comp = fdiv(rest, M, inM), m = rest - comp * M;
         const int za = z0 + 2 * zp, zb = za + 1;
         const C *col = T + ((size_t)(comp * g.N + n) * M + m) * Z;
-        const C va = (za < Z) ? col[za] : CTraits<C>::make(0, 0);
-        const C vb = (zb < Z) ? col[zb] : CTraits<C>::make(0, 0);
+        C va, vb;
+        if (pair16<C>(Z, zb)) {  // both rows in one 16-byte load (FP32, even Z: za even, col 16-byte aligned)
+            const float4 q = *reinterpret_cast<const float4 *>(col + za);
+            va = CTraits<C>::make(q.x, q.y);
+            vb = CTraits<C>::make(q.z, q.w);
+        } else {
+            va = (za < Z) ? col[za] : CTraits<C>::make(0, 0);
+            vb = (zb < Z) ? col[zb] : CTraits<C>::make(0, 0);
+        }
         C *X = bufA + (comp * np + zp) * RS;
         X[M + m] = CTraits<C>::make(0, 0);
         if (m == 0) {
@@ -255,8 +270,12 @@ __device__ __forceinline__ void nl_theta_body(const NLArgs &a, int bx, int by) {
         const C vb = CTraits<C>::make((R)0.5 * (A.y + B.y), (R)-0.5 * (A.x - B.x));
         C *col = T + ((size_t)(comp * g.N + n) * M + m) * Z;
         const int za = z0 + 2 * zp, zb = za + 1;
-        if (za < Z) col[za] = va;
-        if (zb < Z) col[zb] = vb;
+        if (pair16<C>(Z, zb)) {
+            *reinterpret_cast<float4 *>(col + za) = make_float4(va.x, va.y, vb.x, vb.y);
+        } else {
+            if (za < Z) col[za] = va;
+            if (zb < Z) col[zb] = vb;
+        }
     }
 }
 
