@@ -124,9 +124,19 @@ __device__ __forceinline__ void nl_zinv_body(const NLArgs &a, int bx, int by, in
     __syncthreads();
     FR::template run<+1>(rows, mc, tw, tw2);
     C *out = T + ((size_t)(comp * g.N + n) * g.M + m0) * ZL;
-    for (int idx = threadIdx.x; idx < mc * ZL; idx += blockDim.x) {
-        const int c = idx / ZL, j = idx - c * ZL;
-        out[idx] = rows[c * RS + j];
+    if constexpr (sizeof(C) == 8 && ZL % 2 == 0) {
+        // FP32, even length: two z values per 16-byte store (every column
+        // of the intermediate starts on a 16-byte boundary)
+        for (int idx = threadIdx.x; idx < mc * ZL / 2; idx += blockDim.x) {
+            const int c = (2 * idx) / ZL, j = 2 * idx - c * ZL;
+            const C x0 = rows[c * RS + j], x1 = rows[c * RS + j + 1];
+            reinterpret_cast<float4 *>(out)[idx] = make_float4(x0.x, x0.y, x1.x, x1.y);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < mc * ZL; idx += blockDim.x) {
+            const int c = idx / ZL, j = idx - c * ZL;
+            out[idx] = rows[c * RS + j];
+        }
     }
 }
 
@@ -295,9 +305,18 @@ __device__ __forceinline__ void nl_zfwd_body(const NLArgs &a, int bx, int by, in
     const int mc = min(MC, g.M - m0);
     fft4_tables<ZL>(tw, tw2, twz);
     const C *in = T + ((size_t)(comp * g.N + n) * g.M + m0) * ZL;
-    for (int idx = threadIdx.x; idx < mc * ZL; idx += blockDim.x) {
-        const int c = idx / ZL, j = idx - c * ZL;
-        rows[c * RS + j] = in[idx];
+    if constexpr (sizeof(C) == 8 && ZL % 2 == 0) {  // FP32, even length: 16-byte loads
+        for (int idx = threadIdx.x; idx < mc * ZL / 2; idx += blockDim.x) {
+            const int c = (2 * idx) / ZL, j = 2 * idx - c * ZL;
+            const float4 q = reinterpret_cast<const float4 *>(in)[idx];
+            rows[c * RS + j] = CTraits<C>::make(q.x, q.y);
+            rows[c * RS + j + 1] = CTraits<C>::make(q.z, q.w);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < mc * ZL; idx += blockDim.x) {
+            const int c = idx / ZL, j = idx - c * ZL;
+            rows[c * RS + j] = in[idx];
+        }
     }
     __syncthreads();
     FR::template run<-1>(rows, mc, tw, tw2);
