@@ -440,6 +440,17 @@ int pf_batch_set_graphs(pf_batch *b, int on);
 int pf_batch_launches(pf_batch *b, unsigned long long *n);
 /* *staged = 1 when the batch's graphs launch each stage once for all pipes. */
 int pf_batch_staged(pf_batch *b, int *staged);
+/* Form of the stage-batched transform stages.  No counterpart in the
+ * reference (it runs one state per process).  on = 1: each of the three
+ * transform stages (z inverse, theta pass with u x curl(u), z forward) is
+ * one persistent launch whose blocks take the tiles of every pipe, of every
+ * transform length, from one work list (longest lengths first), where every
+ * pipe is in mixed precision with transform lengths up to 192; on = 0 (the
+ * default): one launch per stage and transform length, the lengths' launches
+ * running concurrently.  The numbers are bitwise the same either way; the
+ * autotuner (pipeflow.tune) times both.  A change drops the batch's graphs. */
+int pf_batch_set_worklist(pf_batch *b, int on);
+int pf_batch_get_worklist(pf_batch *b, int *on);
 
 /* ---------------------------------------------------------------- serving */
 /* Requests "advance this state by nsteps timesteps" (time-T maps, e.g. the

@@ -57,6 +57,7 @@ struct pf_batch {
     unsigned long long gn[2][2];
     bool warm;                 // the per-pipe eager step has run (branch graphs)
     bool use_graphs;           // capture steps into graphs (else launch directly)
+    bool worklist;             // transform stages as one work-list launch each
     DevScalars *hsc;           // pinned, one per pipe
     int hsc_cap;
     // event pairs of profiled categories captured into each graph:
@@ -264,6 +265,23 @@ extern "C" int pf_batch_set_graphs(pf_batch *b, int on) {
     return PF_OK;
 }
 
+// on = 1: in the stage-batched form each transform stage is one persistent
+// launch over a work list of every pipe's tiles (where every pipe is in mixed
+// precision with transform lengths up to 192); 0 (default): one launch per
+// stage and transform length.  Results are bitwise the same either way.
+extern "C" int pf_batch_set_worklist(pf_batch *b, int on) {
+    PF_ARG(b, "null batch");
+    if ((on != 0) != b->worklist) batch_graphs_reset(b);
+    b->worklist = on != 0;
+    return PF_OK;
+}
+
+extern "C" int pf_batch_get_worklist(pf_batch *b, int *on) {
+    PF_ARG(b && on, "pf_batch_get_worklist: bad argument");
+    *on = b->worklist ? 1 : 0;
+    return PF_OK;
+}
+
 extern "C" int pf_batch_matrices(pf_batch *b) {
     PF_ARG(b, "null batch");
     batch_graphs_reset(b);
@@ -289,7 +307,7 @@ static bool batch_stageable(const pf_batch *b) {
 // Per-pipe arguments of the stage-batched kernels for both pointer states.
 static int staged_build(pf_batch *b) {
     staged_free(b);
-    PF_TRY(pf_nl_batch_build(b->pipes.data(), b->n, &b->nlb));
+    PF_TRY(pf_nl_batch_build(b->pipes.data(), b->n, b->worklist, &b->nlb));
     PF_TRY(pf_step_batch_build(b->pipes.data(), b->n, &b->stb));
     std::vector<SymArgs> sym(b->n);
     std::vector<DevScalars *> scp(b->n);

@@ -391,7 +391,7 @@ struct StageScope {
 };
 struct pf_nl_batch;
 bool pf_nl_batch_supported(pf_ctx *const *pipes, int n);
-int pf_nl_batch_build(pf_ctx *const *pipes, int n, pf_nl_batch **out);
+int pf_nl_batch_build(pf_ctx *const *pipes, int n, bool worklist, pf_nl_batch **out);
 int pf_nl_batch_launch(pf_nl_batch *b, int state, cudaStream_t st, pf_stage_prof *prof, unsigned long long *nk);
 void pf_nl_batch_free(pf_nl_batch *b);
 struct pf_step_batch;

@@ -974,6 +974,84 @@ __global__ void __launch_bounds__(128) k_nl_mean64_fin_batch(const NLArgs *__res
     if (n < a.g.N) nl_mean64_fin_body(a, n);
 }
 
+// ------------------------------------------------- work-list stage kernels
+// One persistent launch per transform stage for every pipe of a
+// mixed-precision batch, whatever its transform length.  The (pipe, tile)
+// items of the stage sit in one list, longest lengths first; each resident
+// block takes the next item from a device counter (the fetch of the item
+// after it is in flight while the block works) and runs the lone-pipe body
+// of that item's length, so the results are bitwise those of the per-length
+// launches.  The last block to leave resets the counter for the stage's next
+// launch.  FP32 lengths 36 to 192 (every length of the batched mix); the
+// shorter ones hold whole rows in registers and keep their own launches.
+#define PF_NL_WL_LENGTHS(X) X(36) X(48) X(72) X(96) X(144) X(192)
+
+static bool wl_length_ok(int L) {
+    switch (L) {
+#define PF_CASE(L) case L:
+        PF_NL_WL_LENGTHS(PF_CASE)
+#undef PF_CASE
+        return true;
+    default:
+        return false;
+    }
+}
+
+// One item of stage ST (0 z inverse, 1 theta pass, 2 z forward) for one
+// length: l = the block index within the pipe's own grid of that stage.  Not
+// inlined, so each length's body gets the register allocation of its own
+// per-length kernel instead of sharing one across every length.
+template <int ST, int L>
+__device__ __noinline__ void nl_wl_run(const NLArgs *__restrict__ args, int pipe, int l) {
+    const NLArgs a = args[pipe];  // by value: stores through its pointers cannot alias it
+    if constexpr (ST == 1) {
+        const int gx = (a.g.Z + a.ZC - 1) / a.ZC;
+        nl_theta_body<L, float2>(a, l % gx, l / gx);
+    } else {
+        const int gx = (a.g.M + a.MC - 1) / a.MC;
+        const int bx = l % gx, by = (l / gx) % a.g.N, bz = l / (gx * a.g.N);
+        if constexpr (ST == 0) nl_zinv_body<L, float2>(a, bx, by, bz);
+        else nl_zfwd_body<L, float2>(a, bx, by, bz);
+    }
+}
+
+template <int ST> __device__ __forceinline__ void nl_wl_item(const NLArgs *__restrict__ args, int pipe, int l) {
+    const int len = ST == 1 ? args[pipe].g.Th : args[pipe].g.Z;
+    switch (len) {
+#define PF_CASE(L)                            \
+    case L:                                   \
+        nl_wl_run<ST, L>(args, pipe, l);      \
+        break;
+        PF_NL_WL_LENGTHS(PF_CASE)
+#undef PF_CASE
+    }
+}
+
+// ctr[0]: next item; ctr[1]: blocks that have left (both zero between launches)
+template <int ST>
+__global__ void __launch_bounds__(NL_THREADS, ST == 1 ? 6 : 5)
+    k_nl_stage_wl(const NLArgs *__restrict__ args, const int2 *__restrict__ items, int nitems, unsigned *ctr) {
+    __shared__ int next[2];
+    if (threadIdx.x == 0) next[0] = (int)atomicAdd(&ctr[0], 1u);
+    __syncthreads();
+    int slot = 0, cur = next[0];
+    while (cur < nitems) {
+        if (threadIdx.x == 0) next[slot ^ 1] = (int)atomicAdd(&ctr[0], 1u);
+        const int2 pb = items[cur];
+        nl_wl_item<ST>(args, pb.x, pb.y);
+        __syncthreads();  // the item's shared memory is free, next[slot ^ 1] is visible
+        slot ^= 1;
+        cur = next[slot];
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();  // this block's last fetch is done before it counts itself out
+        if (atomicAdd(&ctr[1], 1u) == gridDim.x - 1) {
+            ctr[0] = 0u;
+            ctr[1] = 0u;
+        }
+    }
+}
+
 // shared-memory limit of the mean-mode partial-sum kernels (up to N = 128)
 static int mean_attrs() {
     static bool set = false;
@@ -1013,6 +1091,13 @@ struct pf_nl_batch {
     std::vector<NLGroup> fgroups;
     cudaStream_t faux[NLB_MAXG];
     cudaEvent_t ffork, fjoin[NLB_MAXG];
+    // work-list form (pf_batch_set_worklist): one persistent launch per
+    // stage over the items of every group, in the groups' order
+    bool wl;
+    int2 *wl_items[NLB_STAGES];
+    int wl_n[NLB_STAGES], wl_grid[NLB_STAGES];
+    size_t wl_smem[NLB_STAGES];
+    unsigned *wl_ctr;  // two counters per stage
 };
 
 bool pf_nl_batch_supported(pf_ctx *const *pipes, int n) {
@@ -1033,6 +1118,8 @@ void pf_nl_batch_free(pf_nl_batch *b) {
     }
     cudaFree(b->mean_blk);
     cudaFree(b->fin_blk);
+    for (int st = 0; st < NLB_STAGES; ++st) cudaFree(b->wl_items[st]);
+    cudaFree(b->wl_ctr);
     for (NLGroup &gr : b->fgroups) cudaFree(gr.blk);
     if (b->ffork) cudaEventDestroy(b->ffork);
     for (int k = 0; k < NLB_MAXG; ++k) {
@@ -1142,8 +1229,49 @@ static int nlb_groups(pf_nl_batch *b, pf_ctx *const *pipes, int n) {
     return upload(&b->fin_blk, fin);
 }
 
-// Arguments of every pipe in both pointer states, and the per-group maps.
-int pf_nl_batch_build(pf_ctx *const *pipes, int n, pf_nl_batch **out) {
+template <int ST> static int wl_plan(pf_nl_batch *b, int dev_sms) {
+    static size_t set_ = 0;
+    PF_TRY(raise_smem(k_nl_stage_wl<ST>, b->wl_smem[ST], set_));
+    int per_sm = 0;
+    PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nl_stage_wl<ST>, NL_THREADS, b->wl_smem[ST]));
+    if (per_sm < 1) {
+        pf_set_error("batched transforms: work-list stage %d does not fit an SM", ST);
+        return PF_ERR_ARG;
+    }
+    b->wl_grid[ST] = std::min(b->wl_n[ST], per_sm * dev_sms);
+    return PF_OK;
+}
+
+// The work-list form of the three stages, when every three-pass group is in
+// FP32 with a length the work-list kernels are built for; otherwise the
+// batch keeps the per-length launches.
+static int nlb_worklists(pf_nl_batch *b, pf_ctx *const *pipes, int n) {
+    for (int st = 0; st < NLB_STAGES; ++st)
+        for (const NLGroup &gr : b->groups[st])
+            if (!gr.mixed || !wl_length_ok(gr.L)) return PF_OK;
+    PF_CUDA(cudaMalloc((void **)&b->wl_ctr, 2 * NLB_STAGES * sizeof(unsigned)));
+    PF_CUDA(cudaMemset(b->wl_ctr, 0, 2 * NLB_STAGES * sizeof(unsigned)));
+    int dev = 0, sms = 0;
+    PF_CUDA(cudaGetDevice(&dev));
+    PF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    for (int st = 0; st < NLB_STAGES; ++st) {
+        std::vector<int2> items;
+        size_t smem = 0;
+        for (const NLGroup &gr : b->groups[st]) nlb_group_map<float2>(st, gr.L, true, pipes, n, items, smem);
+        b->wl_n[st] = (int)items.size();
+        b->wl_smem[st] = smem;
+        PF_TRY(upload(&b->wl_items[st], items));
+    }
+    PF_TRY(wl_plan<0>(b, sms));
+    PF_TRY(wl_plan<1>(b, sms));
+    PF_TRY(wl_plan<2>(b, sms));
+    b->wl = true;
+    return PF_OK;
+}
+
+// Arguments of every pipe in both pointer states, and the per-group maps
+// (and the work lists, when asked for and every group qualifies).
+int pf_nl_batch_build(pf_ctx *const *pipes, int n, bool worklist, pf_nl_batch **out) {
     *out = nullptr;
     if (!pf_nl_batch_supported(pipes, n)) {
         pf_set_error("batched transforms: a transform length is not built");
@@ -1162,6 +1290,7 @@ int pf_nl_batch_build(pf_ctx *const *pipes, int n, pf_nl_batch **out) {
         s = upload(&b->d_args[st], h);
     }
     if (s == PF_OK) s = nlb_groups(b, pipes, n);
+    if (s == PF_OK && worklist) s = nlb_worklists(b, pipes, n);
     int ng = 0;
     for (int st = 0; st < NLB_STAGES; ++st) ng = std::max(ng, (int)b->groups[st].size());
     for (int st = 0; st < NLB_STAGES && s == PF_OK; ++st) {
@@ -1229,6 +1358,18 @@ static int nlb_fused_launch(const NLGroup &gr, const NLArgs *args, cudaStream_t 
 
 // one stage: the first group on st, the others forked onto auxiliary streams
 static int nlb_stage(pf_nl_batch *b, int stage, const NLArgs *args, cudaStream_t st, unsigned long long *nk) {
+    if (b->wl) {
+        if (b->wl_n[stage] == 0) return PF_OK;
+        const int g = b->wl_grid[stage], n = b->wl_n[stage];
+        const size_t sm = b->wl_smem[stage];
+        unsigned *ctr = b->wl_ctr + 2 * stage;
+        if (stage == 0) k_nl_stage_wl<0><<<g, NL_THREADS, sm, st>>>(args, b->wl_items[0], n, ctr);
+        else if (stage == 1) k_nl_stage_wl<1><<<g, NL_THREADS, sm, st>>>(args, b->wl_items[1], n, ctr);
+        else k_nl_stage_wl<2><<<g, NL_THREADS, sm, st>>>(args, b->wl_items[2], n, ctr);
+        PF_CHECK_LAUNCH();
+        ++*nk;
+        return PF_OK;
+    }
     const std::vector<NLGroup> &gs = b->groups[stage];
     if (gs.size() > 1) {
         PF_CUDA(cudaEventRecord(b->fork[stage], st));

@@ -191,6 +191,8 @@ _SIGS = {
                        C.POINTER(C.c_longlong)],
     "pf_serve_batch": [P, PP],
     "pf_batch_staged": [P, C.POINTER(I)],
+    "pf_batch_set_worklist": [P, I],
+    "pf_batch_get_worklist": [P, C.POINTER(I)],
     "pf_ctx_launches": [P, C.POINTER(C.c_ulonglong)],
     "pf_prof_enable": [P, I],
     "pf_prof_read": [P, I, DP, C.POINTER(C.c_ulonglong)],

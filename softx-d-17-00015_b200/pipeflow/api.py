@@ -600,6 +600,18 @@ class Batch:
         """False: launch every step directly (membership changing every step)."""
         _check(self.lib.pf_batch_set_graphs(self.h, int(bool(on))))
 
+    @property
+    def worklist(self) -> bool:
+        """Whether each transform stage runs as one persistent launch over a
+        work list of every pipe's tiles (else one launch per transform length)."""
+        v = C.c_int()
+        _check(self.lib.pf_batch_get_worklist(self.h, C.byref(v)))
+        return bool(v.value)
+
+    def set_worklist(self, on: bool):
+        """Choose the form of the transform stages (bitwise the same results)."""
+        _check(self.lib.pf_batch_set_worklist(self.h, int(bool(on))))
+
     def matrices(self):
         _check(self.lib.pf_batch_matrices(self.h))
 

@@ -14,7 +14,10 @@ length.  Here the choices are those pf_ctx_set_tuning exposes:
              one radial point in one block (1);
   nl_mc      columns (azimuthal modes m) per block of the z transform passes
              (not timed where one block per radial point runs);
-  nl_zc      z rows per block of the theta pass (two rows per complex FFT).
+  nl_zc      z rows per block of the theta pass (two rows per complex FFT);
+  worklist   (a batch as a whole) the transform stages as one launch per
+             stage and transform length, or one persistent launch per stage
+             over a work list of every pipe's tiles (pf_batch_set_worklist).
 
 Every choice gives the same numbers bit for bit, so the tuner only times
 them.  It times timesteps in the steporbit form (exactly one corrector per
@@ -22,7 +25,8 @@ step, so every candidate does the same work), by coordinate descent: the
 solver first, then the z tile, then the theta tile, each with the others
 held (then the transform form, then the tiles).  A pipe is tuned on its own; a batch is tuned shape by shape (pipes of
 one (N, K, M, Mp, precision) share a choice) while the whole batch steps,
-since the kernels of different shapes share the GPU.  Choices are cached in
+since the kernels of different shapes share the GPU, and then the form of its
+transform stages.  Choices are cached in
 a JSON file (PIPEFLOW_TUNE_CACHE, default ~/.cache/pipeflow_b200/tuning.json)
 keyed by the pipe shape, or by the batch's shape multiset.
 
@@ -43,6 +47,7 @@ ZC_CANDIDATES = (0, 4, 8, 16, 32)
 LD_CANDIDATES = (L.PF_LD_AUTO, L.PF_LD_WARPRING, L.PF_LD_REBUILT, L.PF_LD_PAIRED)
 KNOBS = ("ld_solver", "nl_fused", "nl_mc", "nl_zc")
 DEFAULT = {"ld_solver": L.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 0, "nl_fused": 0}
+WORKLIST_KEY = "batch"  # batch-wide choices in a batch's cache entry
 
 
 def _candidates(knob: str, shape) -> tuple:
@@ -190,10 +195,12 @@ class Tuner:
         sig = "batch:" + ",".join(f"{_shape_key(s)}x{len(v)}" for s, v in sorted(shapes.items()))
         if self.use_cache:
             hit = self._load().get(sig)
-            if hit and set(hit) == {_shape_key(s) for s in shapes}:
+            if hit and set(hit) - {WORKLIST_KEY} == {_shape_key(s) for s in shapes}:
                 for s, pipes in shapes.items():
                     for p in pipes:
                         p.set_tuning(**hit[_shape_key(s)])
+                if WORKLIST_KEY in hit and hasattr(batch, "set_worklist"):
+                    batch.set_worklist(bool(hit[WORKLIST_KEY]["worklist"]))
                 return hit
         snap = _Snapshot(batch.pipes)
         choice = {s: dict(DEFAULT) for s in shapes}
@@ -222,7 +229,13 @@ class Tuner:
                         p.set_tuning(**new)
                     choice[s] = new
                 self._best(values, apply, run)
+        # the batch-wide form of the transform stages, with every shape's
+        # choices held: per-length launches or one work-list launch per stage
+        if hasattr(batch, "set_worklist"):
+            self._best((False, True), batch.set_worklist, run)
         snap.restore()
         out = {_shape_key(s): c for s, c in choice.items()}
+        if hasattr(batch, "set_worklist"):
+            out[WORKLIST_KEY] = {"worklist": int(batch.worklist)}
         self._store(sig, out)
         return out

@@ -76,6 +76,55 @@ def test_batch_equals_lone_pipes(variant):
     batch.close()
 
 
+@pytest.mark.parametrize("orbit", [False, True], ids=["main", "orbit"])
+def test_batch_worklist_stages_equal_lone_pipes(orbit):
+    """Mixed precision with each transform stage as one persistent launch over
+    a work list of every pipe's tiles (all four transform lengths of each
+    pass in one launch): bitwise the lone pipes, and one launch per stage."""
+    import pipeflow as P
+    cfgs = _cfgs(P.PF_PREC_MIXED)
+    batch = P.Batch(cfgs)
+    batch.set_worklist(True)
+    assert batch.worklist
+    batch.matrices()
+    alone = [P.Pipe(c) for c in cfgs]
+    for i, (bp, ap) in enumerate(zip(batch.pipes, alone)):
+        ap.vel_matrices()
+        _seed(bp, i)
+        _seed(ap, i)
+    batch.step(1, orbit=orbit)  # eager first step
+    n0 = batch.launches()
+    batch.step(4, orbit=orbit)
+    assert batch.staged()
+    for ap in alone:
+        if orbit:
+            ap.steporbit(5)
+        else:
+            for _ in range(5):
+                ap.timestep()
+    for bp, ap in zip(batch.pipes, alone):
+        for (br, bi), (ar, ai) in zip(bp.get_state(), ap.get_state()):
+            assert np.array_equal(br, ar) and np.array_equal(bi, ai)
+        assert bp.tim.step == ap.tim.step == 5
+    n_wl = batch.launches() - n0
+    # switching back rebuilds the per-length launches; still the lone pipes
+    batch.set_worklist(False)
+    batch.step(1, orbit=True)  # eager first step of the rebuilt launches
+    n1 = batch.launches()
+    batch.step(4, orbit=True)
+    n_pl = batch.launches() - n1
+    for ap in alone:
+        ap.steporbit(5)
+    for bp, ap in zip(batch.pipes, alone):
+        for (br, bi), (ar, ai) in zip(bp.get_state(), ap.get_state()):
+            assert np.array_equal(br, ar) and np.array_equal(bi, ai)
+    if orbit:
+        # the three work-list launches of an evaluation replace one launch per
+        # stage and transform length
+        assert n_wl < n_pl, (n_wl, n_pl)
+    batch.close()
+
+
 def test_batch_staged_launch_count():
     """A stage-batched step is a fixed number of launches, whatever the pipe count."""
     import pipeflow as P

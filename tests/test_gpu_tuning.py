@@ -141,7 +141,8 @@ def test_autotuned_batch_equals_untuned(tmp_path):
     a, b = _batch(mix), _batch(mix)
     tuner = P.Tuner(cache_path=tmp_path / "tuning.json", steps=2, reps=1)
     choice = tuner.tune_batch(a)
-    assert len(choice) == 4 and len(tuner.log) > 8
+    assert len(choice) == 5 and len(tuner.log) > 8
+    assert choice["batch"]["worklist"] in (0, 1) and a.worklist == bool(choice["batch"]["worklist"])
     for pa, pb in zip(a.pipes, b.pipes):
         assert _states_equal(pa, pb)
         assert pa.tim.step == pb.tim.step

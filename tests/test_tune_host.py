@@ -73,6 +73,34 @@ class FakeBatch:
         pass
 
 
+class FakeWorklistBatch(FakeBatch):
+    """A batch whose work-list form of the transform stages is faster."""
+
+    def __init__(self, pipes):
+        super().__init__(pipes)
+        self.worklist = False
+
+    def set_worklist(self, on):
+        self.worklist = bool(on)
+
+    def step(self, n, orbit=False):
+        super().step(n, orbit)
+        if not self.worklist:
+            FakePipe.clock[0] += n * 5.0
+
+
+def test_batch_tuning_times_the_work_list_form_and_caches_it(tmp_path, monkeypatch):
+    monkeypatch.setattr(T.time, "perf_counter", lambda: FakePipe.clock[0])
+    best = {"ld_solver": P.PF_LD_AUTO, "nl_mc": 0, "nl_zc": 16, "nl_fused": 0}
+    batch = FakeWorklistBatch([FakePipe(48, 32, 24, 0, best), FakePipe(48, 32, 24, 0, best)])
+    cache = tmp_path / "tuning.json"
+    choice = T.Tuner(cache_path=cache, steps=2, reps=1).tune_batch(batch)
+    assert choice == {"N48K32M24Mp1fp64": best, "batch": {"worklist": 1}} and batch.worklist
+    batch.set_worklist(False)
+    again = T.Tuner(cache_path=cache, steps=2, reps=1)
+    assert again.tune_batch(batch) == choice and again.log == [] and batch.worklist
+
+
 def test_split_is_only_tried_in_mixed_precision_and_the_one_pass_kernel_skips_the_z_tile():
     assert T._candidates("nl_fused", (32, 16, 12, 1, P.PF_PREC_MIXED)) == (0, 1)
     assert T._candidates("nl_fused", (32, 16, 12, 1, P.PF_PREC_FP64)) == (0,)
