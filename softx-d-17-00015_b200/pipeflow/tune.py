@@ -14,7 +14,9 @@ length.  Here the choices are those pf_ctx_set_tuning exposes:
              one radial point in one block (1);
   nl_mc      columns (azimuthal modes m) per block of the z transform passes
              (not timed where one block per radial point runs);
-  nl_zc      z rows per block of the theta pass (two rows per complex FFT);
+  nl_zc      z rows per block of the theta pass (two rows per complex FFT;
+             the candidates include the tiles whose rows fill the passes of
+             the four-step row transform);
   worklist   (a batch as a whole) the transform stages as one launch per
              stage and transform length, or one persistent launch per stage
              over a work list of every pipe's tiles (pf_batch_set_worklist).
@@ -57,7 +59,36 @@ def _candidates(knob: str, shape) -> tuple:
         return (0, 1) if shape[4] == L.PF_PREC_MIXED else (0,)
     if knob == "nl_mc":
         return tuple(_mc_candidates(shape[2]))
-    return ZC_CANDIDATES
+    return _zc_candidates(3 * shape[2])
+
+
+def _fft4_l1(L: int) -> int:
+    """The first factor of the four-step split of a length-L row FFT (the
+    kernels' fft4_l1): L itself up to 32, else the largest divisor d with
+    d * d <= L and L / d <= 32."""
+    if L <= 32:
+        return L
+    best = 0
+    for d in range(1, 33):
+        if L % d == 0 and L // d <= 32 and (best == 0 or (d * d <= L and d > best) or (best * best > L and d < best)):
+            best = d
+    return best
+
+
+def _zc_candidates(Th: int) -> tuple:
+    """Theta-pass tiles to time: the fixed set, plus the even tiles whose
+    3 * ZC complex rows fill one, two or three passes of the four-step
+    transform's two steps (a 256-thread block takes 256 // L2 rows at a time
+    in the first step and 256 // L1 in the second), so no pass runs part-empty."""
+    out = set(ZC_CANDIDATES)
+    L1 = _fft4_l1(Th)
+    per_pass = {256 // (Th // L1), 256 // L1} if L1 < Th else {256}
+    for per in per_pass:
+        for passes in (1, 2, 3):
+            zc = (per * passes // 3) // 2 * 2
+            if 2 <= zc <= 32:
+                out.add(zc)
+    return tuple(sorted(out))
 
 
 def _fused_applies(pipe, cur: dict) -> bool:

@@ -14,6 +14,12 @@ def test_tile_candidates_cover_the_built_in_and_the_whole_range():
         assert c[0] == 0 and M in c and all(1 <= x <= M for x in c[1:])
         assert c == sorted(set(c))
     assert 0 in T.ZC_CANDIDATES and all(z % 2 == 0 for z in T.ZC_CANDIDATES)
+    # the kernels' four-step split, and theta tiles that fill its passes
+    assert [T._fft4_l1(L) for L in (12, 36, 72, 96, 144, 192, 288)] == [12, 6, 8, 8, 12, 12, 16]
+    assert T._zc_candidates(36) == (0, 4, 8, 14, 16, 28, 32)
+    for Th in (36, 48, 72, 96, 144, 192):
+        c = T._zc_candidates(Th)
+        assert set(T.ZC_CANDIDATES) <= set(c) and all(z % 2 == 0 and 0 <= z <= 32 for z in c)
 
 
 class _Cfg:
