@@ -199,11 +199,14 @@ static int ctx_init(pf_ctx *ctx, const pf_config *cfg, int device) {
     PF_TRY(pf_alloc(ctx, &ctx->T, ctx->T_bytes));
     // LU factor storage for the four matrix sets
     pf_lumesh *L[4] = {&ctx->LNp, &ctx->LDp, &ctx->LDm, &ctx->LDz};
+    const int Hcp = pf_compact_modes_padded(g);
     for (pf_lumesh *A : L) {
         A->ctx = ctx;
         PF_TRY(pf_alloc(ctx, (void **)&A->lu, (size_t)NLU * N * g.Hp * sizeof(double)));
         PF_TRY(pf_alloc(ctx, (void **)&A->piv, (size_t)N * g.Hp));
         PF_TRY(pf_alloc(ctx, (void **)&A->pivd, (size_t)N * g.Hp * sizeof(double)));
+        PF_TRY(pf_alloc(ctx, (void **)&A->luc, (size_t)NLU * N * Hcp * sizeof(double)));
+        PF_TRY(pf_alloc(ctx, (void **)&A->pivdc, (size_t)N * Hcp * sizeof(double)));
     }
     ctx->Ltp.ctx = ctx->Ltm.ctx = ctx->Ltz.ctx = ctx;
     // tim_precompute (timestep.f90:29-40)

@@ -260,9 +260,54 @@ __device__ __forceinline__ void fft4_tables(C *tw, C *tw2, const C *__restrict__
 }
 
 // ---------------------------------------------------------------------------
+// Stockham passes of radix 8 or 6 where the length allows (else as above),
+// each butterfly an in-register codelet (rfft_run): a length-384 row takes
+// three passes (8, 8, 6) instead of five (4, 4, 4, 2, 3), so three barriers
+// and shared-memory round trips instead of five.
+__host__ __device__ constexpr int fft_big_radix(int L) {
+    return L % 8 == 0 ? 8 : L % 6 == 0 ? 6 : fft_first_radix(L);
+}
+
+template <int L, int R, int NS, int SIGN, typename C>
+__device__ __forceinline__ void fft_pass_big(const C *__restrict__ src, C *__restrict__ dst, int B, const C *tw) {
+    constexpr int NB = L / R;
+    constexpr int STRIDE = L / (NS * R);
+    for (int idx = threadIdx.x; idx < NB * B; idx += blockDim.x) {
+        const int b = idx / NB, j = idx - b * NB;
+        const int k = j % NS;
+        const C *sp = src + b * L;
+        C *dp = dst + b * L;
+        C v[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            C x = sp[j + q * NB];
+            if (NS > 1 && q > 0) x = c_mul(x, c_tw<SIGN>(tw[q * k * STRIDE]));
+            v[q] = x;
+        }
+        if constexpr (R == 8 || R == 6) rfft_run<R, R, 1, SIGN>(v, tw, L / R);
+        else fft_dft<R, SIGN>(v, tw, L);
+        const int base = (j / NS) * NS * R + k;
+#pragma unroll
+        for (int q = 0; q < R; ++q) dp[base + q * NS] = v[q];
+    }
+}
+
+template <int L, int REM, int NS, int SIGN, typename C>
+__device__ __forceinline__ C *fft_run_big(C *src, C *dst, int B, const C *tw) {
+    if constexpr (REM == 1) {
+        return src;
+    } else {
+        constexpr int R = fft_big_radix(REM);
+        fft_pass_big<L, R, NS, SIGN>(src, dst, B, tw);
+        __syncthreads();
+        return fft_run_big<L, REM / R, NS * R, SIGN>(dst, src, B, tw);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Per-length choice between the four-step transform (one shared-memory
 // transpose, codelets in registers) and the multi-pass Stockham transform
-// (a ping-pong buffer of B*L, low register use).  FP64 lengths above 192
+// (a ping-pong buffer of B*L, radix-8/6 register codelets, low register use).  FP64 lengths above 192
 // need ~165 registers per thread in the four-step form, which caps occupancy
 // at one 256-thread block per SM; they use Stockham.
 template <int L, typename C> struct FFTRows {
@@ -276,7 +321,7 @@ template <int L, typename C> struct FFTRows {
         if constexpr (four) {
             fft4_rows<L, SIGN>(rows, B, pitch, tw, tw2);
         } else {
-            C *res = fft_run<L, L, 1, SIGN>(rows, rows + B * L, B, tw);
+            C *res = fft_run_big<L, L, 1, SIGN>(rows, rows + B * L, B, tw);
             if (res != rows) {
                 for (int i = threadIdx.x; i < B * L; i += blockDim.x) rows[i] = res[i];
                 __syncthreads();

@@ -69,6 +69,15 @@ __host__ __device__ inline void mode_km(int nh, int K, int &k, int &m) {
     }
 }
 
+// Compact index of the modes with k >= 0 (c = m*K + |k|, M*K of them), the
+// layout of the factor copies the streamed solves read, and its padded size.
+__host__ __device__ inline int mode_compact(int nh, int K) {
+    int k = 0, m = 0;
+    mode_km(nh, K, k, m);
+    return m * K + (k < 0 ? -k : k);
+}
+inline int pf_compact_modes_padded(const Geo &g) { return (g.M * g.K + 31) / 32 * 32; }
+
 // Radial mesh on the device (meshs.f90:48-55).
 struct DevMesh {
     const double *rp;      // r^j, j=-3..3: rp[(j+3)*N + n]
@@ -152,6 +161,13 @@ struct pf_lumesh {
     double c1, c2;
     double *lu;
     unsigned char *piv;
+    // context sets only: the factors and pivots (as doubles) of the modes
+    // with k >= 0, [(row*N + col)*Hcp + c] and [col*Hcp + c] with
+    // c = m*K + |k|.  The matrix of mode (-k, m) is bitwise that of (k, m)
+    // (k enters as alpha*k*alpha*k only, timestep.f90:76), so its factors are
+    // too; the streamed solves read this copy and fetch half the factor bytes.
+    double *luc;
+    double *pivdc;
 };
 
 struct pf_ctx {

@@ -360,6 +360,26 @@ __global__ void k_piv_to_double(const unsigned char *__restrict__ piv, double *_
         pivd[i] = (double)piv[i];
 }
 
+// The compact copy of a factor set: the band and pivots of the modes with
+// k >= 0 only, at c = m*K + k (padding columns zero).
+__global__ void k_lu_compact(const double *__restrict__ lu, const double *__restrict__ pivd, double *__restrict__ luc,
+                             double *__restrict__ pivdc, int N, int Hp, int Hcp, int K, int M) {
+    const size_t rows = (size_t)NLU * N + N;  // band entries, then the pivot row of each column
+    const size_t total = rows * Hcp;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = i / Hcp;
+        const int c = (int)(i - r * Hcp);
+        double v = 0.0;
+        if (c < M * K) {
+            const int m = c / K, k = c - m * K;
+            const int nh = m == 0 ? k : m * (2 * K - 1) + k;
+            v = r < (size_t)NLU * N ? lu[r * Hp + nh] : pivd[(r - (size_t)NLU * N) * Hp + nh];
+        }
+        if (r < (size_t)NLU * N) luc[r * Hcp + c] = v;
+        else pivdc[(r - (size_t)NLU * N) * Hcp + c] = v;
+    }
+}
+
 static int lumesh_init(pf_ctx *ctx, pf_lumesh *A, int PM, int BC, double c1, double c2) {
     A->PM = PM;
     A->BC = BC;
@@ -367,12 +387,23 @@ static int lumesh_init(pf_ctx *ctx, pf_lumesh *A, int PM, int BC, double c1, dou
     A->c2 = c2;
     PF_TRY(pf_launch_lu_factor(ctx, A));
     if (A->pivd) {  // pivots as doubles, staged by the fused solves with 8-byte copies
-        const size_t np = (size_t)ctx->g.N * ctx->g.Hp;
+        const Geo &g = ctx->g;
+        const size_t np = (size_t)g.N * g.Hp;
         {
             ProfScope ps_(ctx, PF_K_FACTOR);
             k_piv_to_double<<<grid1(np, 256), 256, 0, ctx->stream>>>(A->piv, A->pivd, np);
         }
         PF_LAUNCHED(ctx);
+        if (A->luc) {
+            const int Hcp = pf_compact_modes_padded(g);
+            const size_t nc = ((size_t)NLU * g.N + g.N) * Hcp;
+            {
+                ProfScope ps_(ctx, PF_K_FACTOR);
+                k_lu_compact<<<grid1(nc, 256), 256, 0, ctx->stream>>>(A->lu, A->pivd, A->luc, A->pivdc, g.N, g.Hp, Hcp,
+                                                                      g.K, g.M);
+            }
+            PF_LAUNCHED(ctx);
+        }
     }
     return PF_OK;
 }

@@ -63,7 +63,9 @@ unsigned long long bytes_estimate(const pf_config &c) {
     b += 23 * coll;                            // vel, prev, save, scratch
     b += 6 * phys;                             // physical fields
     b += 6ull * N * c.M * Z * 16;              // transform intermediate
+    const unsigned long long Hcp = (1ull * c.M * c.K + 31) / 32 * 32;
     b += 4 * (NLU * N * Hp * 8 + N * Hp + N * Hp * 8);  // four factor sets, pivots
+    b += 4 * (NLU * N * Hcp * 8 + N * Hcp * 8);          // their compact (k >= 0) copies
     b += 6 * N * Hp * 8 + 16 * Hp * 8;         // influence vectors and 4x4 inverses
     b += 64 * N * 8 + 4 * (Z + Th) * 16;       // mesh, twiddles, small buffers
     return b;

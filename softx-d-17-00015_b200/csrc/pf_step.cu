@@ -37,6 +37,11 @@ struct StepArgs {
     const double *pivd;    // LNp pivots as doubles [col*Hp + nh]
     const double *pivld[3];  // LDp/LDm/LDz pivots as doubles
     int ldpiv[3];          // 1 if that Helmholtz factorisation pivoted
+    // compact copies (modes k >= 0, c = m*K + |k|, stride Hcp) the streamed
+    // pressure and Helmholtz solves read: LNp, LDp, LDm, LDz and their pivots
+    const double *lnpc, *ldc[3];
+    const double *pivdc, *pivldc[3];
+    int Hcp;
     double ldc1, ldc2;     // Helmholtz coefficients (LDp/LDm/LDz: 1/dt, -implicit nu/Re)
     const double *U, *Ainv, *Ui;
     DevMesh dm;
@@ -748,8 +753,9 @@ __device__ __forceinline__ void solve_pnpw_body(const StepArgs &a, int bx) {
     }
     if (!live) return;
     const double *rhs = reinterpret_cast<const double *>(a.prhs) + 2 * (size_t)nh + part;
-    solve_async_rw<true>(a.lnp, a.pivd, g.N, g.Hp, nh, rhs, st, out, st, ring2w + (size_t)w * RING * rw_slot<true>(),
-                         mask);
+    // factors of the compact copy: mode (-k, m) reads those of (k, m)
+    solve_async_rw<true>(a.lnpc, a.pivdc, g.N, a.Hcp, mode_compact(nh, g.K), rhs, st, out, st,
+                         ring2w + (size_t)w * RING * rw_slot<true>(), mask);
 }
 
 // S4 with the shared rings: warp = one system of 16 consecutive modes x (re,
@@ -850,11 +856,14 @@ __device__ __forceinline__ void solve_ld_body(const StepArgs &a, int bx) {
     const size_t st = 2 * (size_t)g.Hp;
     const double *rhs = reinterpret_cast<const double *>(pick3(a.rl, sys)) + 2 * (size_t)nh + part;
     double *out = reinterpret_cast<double *>(pick3(a.v, sys)) + 2 * (size_t)nh + part;
-    const double *lu = sys == 0 ? a.ldp : sys == 1 ? a.ldm : a.ldz;
+    // factors of the compact copy: mode (-k, m) reads those of (k, m), so a
+    // warp's factor loads cover about half as many distinct columns
+    const double *lu = pick3(a.ldc, sys);
+    const int c = mode_compact(nh, g.K);
     if (pick3(a.ldpiv, sys))  // pivoting band (low Re, small dt or very clustered meshes)
-        solve_async<true, 192>(lu, pick3(a.pivld, sys), g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x);
+        solve_async<true, 192>(lu, pick3(a.pivldc, sys), g.N, a.Hcp, c, rhs, st, out, st, ring4 + threadIdx.x);
     else
-        solve_async<false, 192>(lu, nullptr, g.N, g.Hp, nh, rhs, st, out, st, ring4 + threadIdx.x);
+        solve_async<false, 192>(lu, nullptr, g.N, a.Hcp, c, rhs, st, out, st, ring4 + threadIdx.x);
 }
 
 // ------------------------- S4 with the factors rebuilt on chip (no pivoting)
@@ -1306,7 +1315,12 @@ static StepArgs make_step_args(const pf_ctx *ctx, int corrector) {
     for (int i = 0; i < 3; ++i) {
         a.pivld[i] = ld[i]->pivd;
         a.ldpiv[i] = ld[i]->pivoted;
+        a.ldc[i] = ld[i]->luc;
+        a.pivldc[i] = ld[i]->pivdc;
     }
+    a.lnpc = ctx->LNp.luc;
+    a.pivdc = ctx->LNp.pivdc;
+    a.Hcp = pf_compact_modes_padded(ctx->g);
     a.ldc1 = ctx->LDp.c1;
     a.ldc2 = ctx->LDp.c2;
     a.ldp = ctx->LDp.lu;
