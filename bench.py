@@ -471,6 +471,14 @@ def run_batched(args, torch, P, dist, world, rank, local):
     e1.record(master)
     master.synchronize()
     e2e_ms = e0.elapsed_time(e1)
+    # the same copies with no step between them (both directions at once, on
+    # the batch's copy streams): the PCIe rate the end-to-end figure meets
+    t0 = time.perf_counter()
+    for s in range(ne):
+        batch.put_states(s % 2, hin[s % 2])
+        batch.get_states(s % 2, hout[s % 2])
+    batch.io_sync()
+    copies_ms = (time.perf_counter() - t0) * 1e3 / ne
     worklist = batch.worklist
     batch.close()
     S = [coll_bytes(d) for d in cfgs]
@@ -535,6 +543,7 @@ def run_batched(args, torch, P, dist, world, rank, local):
                 e2e_path="pf_batch_put_states / pf_batch_step_io / pf_batch_get_states: one pinned state block "
                          "in and one out per step, copies on their own streams overlapping the step between",
                 extra=extra, dom=dom, dom_ms=dom_ms, dom_n=dom_n, per_launch=per_launch, h2d=io, d2h=io,
+                copies_ms=copies_ms,
                 dtype="mixed: f32 transforms, f64 solves", config=config_of(args))
 
 
@@ -713,6 +722,9 @@ def main():
                     "path": r.get("e2e_path", "")},
             "clocks": r["clk"],
         }
+        if r.get("copies_ms"):
+            line["e2e"]["copies_only_ms_per_step"] = r["copies_ms"]
+            line["e2e"]["copies_only_gbs_each_way"] = r["h2d"] / (r["copies_ms"] / 1e3) / 1e9
         if args.workload == "batched":
             if r["extra"].get("stage_batched"):
                 line["roofline"]["note"] = (

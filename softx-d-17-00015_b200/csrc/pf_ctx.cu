@@ -2,6 +2,8 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <mutex>
+#include <vector>
 #include "pf_internal.cuh"
 
 static thread_local char g_err[512] = "";
@@ -18,6 +20,27 @@ extern "C" const char *pf_last_error(void) { return g_err; }
 extern "C" int pf_version(int *major, int *minor) {
     if (major) *major = 1;
     if (minor) *minor = 0;
+    return PF_OK;
+}
+
+int pf_raise_smem(const void *fn, size_t bytes) {
+    struct Limit {
+        const void *fn;
+        int device;
+        size_t bytes;
+    };
+    static std::mutex mu;
+    static std::vector<Limit> limits;
+    int dev = 0;
+    PF_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    Limit *hit = nullptr;
+    for (Limit &l : limits)
+        if (l.fn == fn && l.device == dev) hit = &l;
+    if (hit && hit->bytes >= bytes) return PF_OK;
+    PF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    if (hit) hit->bytes = bytes;
+    else limits.push_back(Limit{fn, dev, bytes});
     return PF_OK;
 }
 

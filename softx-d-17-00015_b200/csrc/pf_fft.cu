@@ -268,10 +268,7 @@ static int pick_zc(const pf_ctx *ctx, int ncomp) {
     return ZC;
 }
 
-static int set_smem(const void *fn, size_t bytes) {
-    PF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    return PF_OK;
-}
+static int set_smem(const void *fn, size_t bytes) { return pf_raise_smem(fn, bytes); }
 
 int pf_launch_coll2phys(pf_ctx *ctx, int ncomp, const double2 *const *src, double *const *dst) {
     const Geo &g = ctx->g;

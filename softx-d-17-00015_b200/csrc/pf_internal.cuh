@@ -293,6 +293,10 @@ struct ProfScope {
 
 // -------------------------------------------------------------- utilities
 int pf_alloc(pf_ctx *ctx, void **p, size_t bytes);
+// Raise, never lower, a kernel's dynamic shared-memory limit on the current
+// device: a limit lowered for a small launch would no longer cover a larger
+// launch of the same kernel that a CUDA graph captured earlier.
+int pf_raise_smem(const void *fn, size_t bytes);
 int pf_coll_init_storage(pf_ctx *ctx, pf_coll *c);
 int pf_phys_init_storage(pf_ctx *ctx, pf_phys *p);
 inline double bits_to_double(unsigned long long b) {

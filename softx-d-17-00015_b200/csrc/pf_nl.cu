@@ -702,11 +702,12 @@ static NLArgs make_nl_args(pf_ctx *ctx) {
     return a;
 }
 
+// cur: the largest limit this call site asked for; the limit itself is kept
+// per device by pf_raise_smem, which every call consults (a process may
+// drive several devices)
 template <typename K> static int raise_smem(K kernel, size_t bytes, size_t &cur) {
-    if (bytes > cur) {
-        PF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-        cur = bytes;
-    }
+    PF_TRY(pf_raise_smem((const void *)kernel, bytes));
+    cur = std::max(cur, bytes);
     return PF_OK;
 }
 

@@ -210,7 +210,7 @@ extern "C" int pf_tra_coll2phys_noalloc(int N, int K, int M, const double *re, c
     switch (Z) {
 #define PF_CASE(L)                                                                                        \
     case L:                                                                                               \
-        PF_CUDA(cudaFuncSetAttribute(k_na_zinv<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsm)); \
+        PF_TRY(pf_raise_smem((const void *)k_na_zinv<L>, zsm));                                          \
         k_na_zinv<L><<<gz, 256, zsm, st>>>(re, im, T, twz, N, K, M, MC);                                   \
         break;
         PF_NA_LENGTHS(PF_CASE)
@@ -223,7 +223,7 @@ extern "C" int pf_tra_coll2phys_noalloc(int N, int K, int M, const double *re, c
     switch (Th) {
 #define PF_CASE(L)                                                                                         \
     case L:                                                                                                \
-        PF_CUDA(cudaFuncSetAttribute(k_na_thinv<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm)); \
+        PF_TRY(pf_raise_smem((const void *)k_na_thinv<L>, tsm));                                          \
         k_na_thinv<L><<<gt, 256, tsm, st>>>(T, phys, twt, M, Z, ZC);                                        \
         break;
         PF_NA_LENGTHS(PF_CASE)
