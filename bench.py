@@ -657,7 +657,7 @@ def main():
     ap.add_argument("--pipes", type=int, default=64)
     ap.add_argument("--spinup", type=int, default=None)
     ap.add_argument("--ref-steps", type=int, default=64)
-    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--plain-pipes", type=int, default=64)
     ap.add_argument("--err-steps", type=int, default=1000)
     ap.add_argument("--cfg2-spinup", type=int, default=500)
