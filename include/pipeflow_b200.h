@@ -445,7 +445,7 @@ int pf_batch_staged(pf_batch *b, int *staged);
  * transform stages (z inverse, theta pass with u x curl(u), z forward) is
  * one persistent launch whose blocks take the tiles of every pipe, of every
  * transform length, from one work list (longest lengths first), where every
- * pipe is in mixed precision with transform lengths up to 192; on = 0 (the
+ * pipe is in mixed precision with transform lengths from 36 to 192; on = 0 (the
  * default): one launch per stage and transform length, the lengths' launches
  * running concurrently.  The numbers are bitwise the same either way; the
  * autotuner (pipeflow.tune) times both.  A change drops the batch's graphs. */

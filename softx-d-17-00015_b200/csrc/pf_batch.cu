@@ -267,7 +267,7 @@ extern "C" int pf_batch_set_graphs(pf_batch *b, int on) {
 
 // on = 1: in the stage-batched form each transform stage is one persistent
 // launch over a work list of every pipe's tiles (where every pipe is in mixed
-// precision with transform lengths up to 192); 0 (default): one launch per
+// precision with transform lengths from 36 to 192); 0 (default): one launch per
 // stage and transform length.  Results are bitwise the same either way.
 extern "C" int pf_batch_set_worklist(pf_batch *b, int on) {
     PF_ARG(b, "null batch");
