@@ -370,8 +370,8 @@ int pf_state_read(const char *path, int N, int K, int M, int Mp, const double *r
 /* ----------------------------------------------------------------- batches */
 /* Many independent pipes of uneven (N, K, M, Re, alpha, dt) advanced together;
  * one timestep of the batch is a single CUDA graph.  Where every pipe fits
- * the batched kernels (fixed dt, N <= 128, transform lengths <= 192, one
- * precision, mean-mode symmetry only) each stage is one launch over the tiles
+ * the batched kernels (fixed dt, N <= 128, built transform lengths 12 to 384,
+ * either precision, mean-mode symmetry only) each stage is one launch over the tiles
  * of all pipes; otherwise the graph holds one kernel chain per pipe.  Each
  * pipe's arithmetic is the lone-pipe path, so results are the same alone and
  * in the batch.  No single reference routine: this drives the main.f90 loop

@@ -3,8 +3,9 @@
 // Each pipe is a full pf_ctx (its own fields, factors and stream).  One
 // timestep of the whole batch is a single CUDA graph, built one of two ways:
 //
-//  * stage-batched (the usual case: fixed dt, N <= 128, transform lengths up
-//    to 192, one precision, no symmetry beyond the mean-mode one): every stage
+//  * stage-batched (the usual case: fixed dt, N <= 128, built transform
+//    lengths 12 to 384, either precision, no symmetry beyond the mean-mode
+//    one; a transform stage takes one launch per length and precision): every stage
 //    of the step is ONE launch over the tiles of all pipes (a (pipe, tile) map
 //    per stage), so a step of the whole batch is about twenty kernels that
 //    each fill the GPU, whatever the mix of sizes;
