@@ -22,7 +22,8 @@ length.  Here the choices are those pf_ctx_set_tuning exposes:
              over a work list of every pipe's tiles (pf_batch_set_worklist).
 
 Every choice gives the same numbers bit for bit, so the tuner only times
-them.  It times timesteps in the steporbit form (exactly one corrector per
+them.  A candidate replaces a knob's current choice only when it is faster by
+more than a margin (0.5% by default), so timing noise does not move choices.  It times timesteps in the steporbit form (exactly one corrector per
 step, so every candidate does the same work), by coordinate descent: the
 solver first, then the z tile, then the theta tile, each with the others
 held (then the transform form, then the tiles).  A pipe is tuned on its own; a batch is tuned shape by shape (pipes of
@@ -144,11 +145,16 @@ class _Snapshot:
 
 
 class Tuner:
-    def __init__(self, cache_path=None, steps: int = 6, reps: int = 2, use_cache: bool = True):
+    def __init__(self, cache_path=None, steps: int = 6, reps: int = 2, use_cache: bool = True,
+                 margin: float = 0.005):
         self.cache_path = Path(cache_path) if cache_path else default_cache_path()
         self.steps = steps
         self.reps = reps
         self.use_cache = use_cache
+        # a candidate replaces the first option of a knob (the current choice)
+        # only when it is faster by more than this fraction: one shape's choice
+        # moves a batch step by well under a percent, about the timing noise
+        self.margin = margin
         self.log = []  # (what, choice, seconds) of every timing taken
 
     # ------------------------------------------------------------ cache
@@ -171,8 +177,10 @@ class Tuner:
 
     # ---------------------------------------------------------- timing
     def _best(self, options, apply, run):
-        """Apply each option, time run(), keep the fastest (min over reps)."""
-        best, best_t = None, float("inf")
+        """Apply each option, time run() (min over reps), keep the fastest;
+        the first option that runs stays unless another beats it by more
+        than the margin."""
+        best, best_t, first_t = None, float("inf"), None
         for opt in options:
             try:
                 apply(opt)
@@ -180,7 +188,9 @@ class Tuner:
                 continue
             t = min(run() for _ in range(self.reps))
             self.log.append((opt, t))
-            if t < best_t:
+            if first_t is None:
+                best, best_t, first_t = opt, t, t
+            elif t < best_t and t < first_t * (1.0 - self.margin):
                 best, best_t = opt, t
         apply(best)
         return best, best_t

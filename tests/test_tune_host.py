@@ -137,3 +137,22 @@ def test_batch_tuning_picks_each_shapes_fastest_choice_and_caches_it(tmp_path, m
     again = T.Tuner(cache_path=cache, steps=2, reps=1)
     assert again.tune_batch(batch) == choice and again.log == []
     assert [p.tuning for p in pipes] == [best_a, best_a, best_b]
+
+
+def test_a_candidate_within_the_margin_keeps_the_current_choice(monkeypatch):
+    clock = [0.0]
+    monkeypatch.setattr(T.time, "perf_counter", lambda: clock[0])
+    cost = {"a": 1.000, "b": 0.998, "c": 0.90}
+    chosen = []
+
+    def apply(v):
+        chosen.append(v)
+
+    tuner = T.Tuner(cache_path="/nonexistent/tuning.json", reps=1, margin=0.005)
+
+    def run():
+        clock[0] += cost[chosen[-1]]
+        return cost[chosen[-1]]
+
+    assert tuner._best(["a", "b"], apply, run)[0] == "a"      # 0.2% faster: kept the first
+    assert tuner._best(["a", "b", "c"], apply, run)[0] == "c"  # 10% faster: taken
